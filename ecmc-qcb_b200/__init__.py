@@ -1,0 +1,309 @@
+"""Python binding of libqcb.so, the B200 gauge-field hot path of ECMC-QCB.
+
+Mirrors the reference's C++ call surface (src/gauge/GaugeField.h, src/heatbath/heatbath_mpi.h,
+src/flow/gradient_flow.h, src/observables/observables_mpi.h, src/io/ildg.h) over the C ABI in
+include/qcb.h.  Every call runs the CUDA kernels of libqcb.so; there is no CPU path, and loading
+fails loudly when the library is missing or no GPU is visible.
+
+Host link arrays are numpy complex128 of shape (V, 4, 3, 3): sites lexicographic with x fastest
+(the ILDG payload order), then mu = x,y,z,t, then the row-major 3x3 matrix.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqcb.so")
+
+PREC_F64, PREC_F32 = 64, 32
+STORE_18, STORE_12 = 0, 1
+K_HB, K_FLOW, K_PLAQ, K_CLOVER, K_OTHER = range(5)
+
+ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "EIO", -4: "EFORMAT", -5: "ECUDA", -6: "ETIMEOUT", -7: "ERANGE"}
+
+
+class QcbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+_i4 = C.c_int * 4
+_dp = np.ctypeslib.ndpointer(dtype=np.complex128, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+
+
+def exported_symbols():
+    """Names of the C ABI functions declared in include/qcb.h, with their ctypes signatures."""
+    d, i, u32, u64, sz = C.c_double, C.c_int, C.c_uint32, C.c_uint64, C.c_size_t
+    pd, pi = C.POINTER(C.c_double), C.POINTER(C.c_int)
+    return {
+        "qcb_last_error": (C.c_char_p, []),
+        "qcb_version": (C.c_char_p, []),
+        "qcb_launch_count": (u64, []),
+        "qcb_field_create": (i, [_i4, i, i, C.POINTER(_vp)]),
+        "qcb_field_destroy": (i, [_vp]),
+        "qcb_field_info": (i, [_vp, _i4, pi, pi, C.POINTER(sz)]),
+        "qcb_field_stream": (_vp, [_vp]),
+        "qcb_field_set_stream": (i, [_vp, _vp]),
+        "qcb_field_sync": (i, [_vp]),
+        "qcb_field_upload_aos": (i, [_vp, _vp]),
+        "qcb_field_download_aos": (i, [_vp, _vp]),
+        "qcb_field_upload_aos_device": (i, [_vp, _vp]),
+        "qcb_field_download_aos_device": (i, [_vp, _vp]),
+        "qcb_field_copy": (i, [_vp, _vp]),
+        "qcb_cold_start": (i, [_vp]),
+        "qcb_hot_start": (i, [_vp, u64]),
+        "qcb_reunitarize": (i, [_vp]),
+        "qcb_unitarity": (i, [_vp, pd, pd]),
+        "qcb_shift": (i, [_vp, _i4]),
+        "qcb_random_shift": (i, [_vp, u64, u64, i, _i4]),
+        "qcb_hb_subsweep": (i, [_vp, d, i, u64, u32, i, i]),
+        "qcb_hb_sweep": (i, [_vp, d, i, u64, u32]),
+        "qcb_plaquette": (i, [_vp, pd]),
+        "qcb_clover_qe": (i, [_vp, pd, pd]),
+        "qcb_flow_create": (i, [_vp, d, i, i, C.POINTER(_vp)]),
+        "qcb_flow_destroy": (i, [_vp]),
+        "qcb_flow_copy": (i, [_vp, _vp]),
+        "qcb_flow_rk3": (i, [_vp, i]),
+        "qcb_flow_measure": (i, [_vp, _vp, i, i, _vp, _vp]),
+        "qcb_flow_field": (_vp, [_vp]),
+        "qcb_ildg_write": (i, [_vp, C.c_char_p]),
+        "qcb_ildg_read": (i, [_vp, C.c_char_p]),
+        "qcb_ildg_probe": (i, [C.c_char_p, _i4, pi]),
+        "qcb_timing_enable": (i, [_vp, i]),
+        "qcb_timing_read": (i, [_vp, i, C.POINTER(C.c_long), pd]),
+        "qcb_timing_reset": (i, [_vp]),
+        "qcb_diag_staple": (i, [_vp, i, _vp]),
+        "qcb_diag_exp_su3": (i, [_vp, i, d, i, _vp]),
+        "qcb_diag_philox": (i, [C.POINTER(u32), C.POINTER(u32), i, C.POINTER(u32)]),
+    }
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Loads libqcb.so and binds every C ABI symbol (no GPU needed to load)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise ImportError(f"libqcb.so not built at {path}: run ecmc-qcb_b200/build.py")
+        lib = C.CDLL(path)
+        for name, (res, args) in exported_symbols().items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def lib() -> C.CDLL:
+    return load_library()
+
+
+def _check(code: int) -> None:
+    if code != 0:
+        raise QcbError(code, lib().qcb_last_error().decode())
+
+
+def launch_count() -> int:
+    return int(lib().qcb_launch_count())
+
+
+def volume(L) -> int:
+    return int(L[0]) * int(L[1]) * int(L[2]) * int(L[3])
+
+
+class GaugeField:
+    """Device-resident periodic gauge field (reference GaugeField + GeometryCB, one GPU)."""
+
+    def __init__(self, L, prec: int = PREC_F64, store: int = STORE_18, _handle=None, _owner=None):
+        self.L = tuple(int(v) for v in L)
+        self.V = volume(self.L)
+        self.prec, self.store = prec, store
+        self._owner = _owner
+        if _handle is not None:
+            self.h = _handle
+            self._owns = False
+        else:
+            h = _vp()
+            _check(lib().qcb_field_create(_i4(*self.L), int(prec), int(store), C.byref(h)))
+            self.h = h
+            self._owns = True
+
+    def close(self) -> None:
+        if getattr(self, "_owns", False) and self.h:
+            lib().qcb_field_destroy(self.h)
+            self.h = None
+            self._owns = False
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- transfers
+    def upload(self, U: np.ndarray) -> None:
+        U = np.ascontiguousarray(U, dtype=np.complex128)
+        assert U.size == self.V * 36, "expected V*4*3*3 complex entries"
+        _check(lib().qcb_field_upload_aos(self.h, U.ctypes.data))
+
+    def download(self) -> np.ndarray:
+        out = np.empty((self.V, 4, 3, 3), dtype=np.complex128)
+        _check(lib().qcb_field_download_aos(self.h, out.ctypes.data))
+        return out
+
+    def upload_device_ptr(self, ptr: int) -> None:
+        _check(lib().qcb_field_upload_aos_device(self.h, _vp(ptr)))
+
+    def download_device_ptr(self, ptr: int) -> None:
+        _check(lib().qcb_field_download_aos_device(self.h, _vp(ptr)))
+
+    def copy_from(self, other: "GaugeField") -> None:
+        _check(lib().qcb_field_copy(self.h, other.h))
+
+    @property
+    def stream(self) -> int:
+        return lib().qcb_field_stream(self.h) or 0
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(lib().qcb_field_set_stream(self.h, _vp(stream_ptr)))
+
+    def sync(self) -> None:
+        _check(lib().qcb_field_sync(self.h))
+
+    def device_bytes(self) -> int:
+        n = C.c_size_t()
+        _check(lib().qcb_field_info(self.h, _i4(), None, None, C.byref(n)))
+        return n.value
+
+    # -- starts, projections
+    def cold_start(self) -> None:
+        _check(lib().qcb_cold_start(self.h))
+
+    def hot_start(self, seed: int) -> None:
+        _check(lib().qcb_hot_start(self.h, int(seed)))
+
+    def reunitarize(self) -> None:
+        _check(lib().qcb_reunitarize(self.h))
+
+    def unitarity(self):
+        mx, mn = C.c_double(), C.c_double()
+        _check(lib().qcb_unitarity(self.h, C.byref(mx), C.byref(mn)))
+        return mx.value, mn.value
+
+    # -- shift
+    def shift(self, s) -> None:
+        _check(lib().qcb_shift(self.h, _i4(*[int(v) for v in s])))
+
+    def random_shift(self, seed: int, idx: int, max_shift: int = 0):
+        o = _i4()
+        _check(lib().qcb_random_shift(self.h, int(seed), int(idx), int(max_shift), o))
+        return [int(v) for v in o]
+
+    # -- heatbath
+    def hb_subsweep(self, beta, n_hits, seed, sweep, parity, mu) -> None:
+        _check(lib().qcb_hb_subsweep(self.h, float(beta), int(n_hits), int(seed), int(sweep), int(parity), int(mu)))
+
+    def hb_sweep(self, beta, n_hits, seed, sweep) -> None:
+        _check(lib().qcb_hb_sweep(self.h, float(beta), int(n_hits), int(seed), int(sweep)))
+
+    # -- observables
+    def plaquette(self) -> float:
+        p = C.c_double()
+        _check(lib().qcb_plaquette(self.h, C.byref(p)))
+        return p.value
+
+    def clover_qe(self):
+        q, e = C.c_double(), C.c_double()
+        _check(lib().qcb_clover_qe(self.h, C.byref(q), C.byref(e)))
+        return q.value, e.value
+
+    def staple(self, mu: int) -> np.ndarray:
+        out = np.empty((self.V, 3, 3), dtype=np.complex128)
+        _check(lib().qcb_diag_staple(self.h, int(mu), out.ctypes.data))
+        return out
+
+    # -- ILDG
+    def save_ildg(self, path: str) -> None:
+        _check(lib().qcb_ildg_write(self.h, os.fsencode(path)))
+
+    def read_ildg(self, path: str) -> None:
+        _check(lib().qcb_ildg_read(self.h, os.fsencode(path)))
+
+    # -- instrumentation
+    def timing(self, on: bool = True) -> None:
+        _check(lib().qcb_timing_enable(self.h, 1 if on else 0))
+
+    def timing_read(self, kclass: int):
+        n, ms = C.c_long(), C.c_double()
+        _check(lib().qcb_timing_read(self.h, int(kclass), C.byref(n), C.byref(ms)))
+        return n.value, ms.value
+
+    def timing_reset(self) -> None:
+        _check(lib().qcb_timing_reset(self.h))
+
+
+def ildg_probe(path: str):
+    L = _i4()
+    p = C.c_int()
+    _check(lib().qcb_ildg_probe(os.fsencode(path), L, C.byref(p)))
+    return tuple(int(v) for v in L), p.value
+
+
+class GradientFlow:
+    """Wilson flow state (reference GradientFlow, src/flow/gradient_flow.h:11-27)."""
+
+    def __init__(self, field: GaugeField, eps: float = 0.02, prec: int | None = None, store: int | None = None):
+        prec = field.prec if prec is None else prec
+        store = field.store if store is None else store
+        h = _vp()
+        _check(lib().qcb_flow_create(field.h, float(eps), int(prec), int(store), C.byref(h)))
+        self.h = h
+        self.eps = eps
+        self.field = GaugeField(field.L, prec, store, _handle=lib().qcb_flow_field(h), _owner=self)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().qcb_flow_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def copy(self, field: GaugeField) -> None:
+        _check(lib().qcb_flow_copy(self.h, field.h))
+
+    def rk3_step(self, n: int = 1) -> None:
+        _check(lib().qcb_flow_rk3(self.h, int(n)))
+
+    def measure(self, field: GaugeField, n_steps: int, n_rk: int = 1, plaquette: bool = False):
+        """topo_charge_flowed: returns an (n_steps, 3) array of (t, Q, E), and plaquettes if asked."""
+        out = np.empty(3 * n_steps)
+        pl = np.empty(n_steps) if plaquette else None
+        _check(lib().qcb_flow_measure(self.h, field.h, int(n_steps), int(n_rk), out.ctypes.data,
+                                      pl.ctypes.data if pl is not None else None))
+        tqe = out.reshape(n_steps, 3)
+        return (tqe, pl) if plaquette else tqe
+
+
+def exp_su3(Z: np.ndarray, coeff: float, prec: int = PREC_F64) -> np.ndarray:
+    z = np.ascontiguousarray(Z, dtype=np.complex128).reshape(-1, 3, 3)
+    out = np.empty_like(z)
+    _check(lib().qcb_diag_exp_su3(z.ctypes.data, z.shape[0], float(coeff), int(prec), out.ctypes.data))
+    return out
+
+
+def philox(ctr, key, n: int = 1) -> np.ndarray:
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    out = (C.c_uint32 * (4 * n))()
+    _check(lib().qcb_diag_philox(c, k, int(n), out))
+    return np.frombuffer(out, dtype=np.uint32).reshape(n, 4).copy()

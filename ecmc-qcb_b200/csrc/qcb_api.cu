@@ -1,0 +1,781 @@
+// qcb_api.cu -- C ABI of libqcb.so: handles, launches and reductions.
+//
+// One handle = one periodic lattice resident on one GPU (the reference's GaugeField +
+// GeometryCB on one MPI rank with a periodic halo, src/gauge/GaugeField.h:18-62).
+// Kernels are launched on the handle's stream; results return to the host only from
+// calls that produce host values.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <atomic>
+#include <new>
+#include <string>
+
+#include "qcb_internal.h"
+#include "qcb_kernels.cuh"
+
+using namespace qcb;
+
+// ====================================================================== errors
+namespace {
+thread_local std::string g_err;
+std::atomic<uint64_t> g_launches{0};
+}  // namespace
+
+int qcb::fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) return fail(QCB_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+#define RET(call)                \
+    do {                         \
+        int r_ = (call);         \
+        if (r_ != QCB_OK) return r_; \
+    } while (0)
+
+// Format dispatch: instantiates BODY with R / NE for the field's storage format.
+#define DISPATCH_FMT(fmt, ...)                \
+    switch (fmt) {                            \
+        case FMT_D18: {                       \
+            typedef double R;                 \
+            constexpr int NE = 9;             \
+            __VA_ARGS__;                      \
+        } break;                              \
+        case FMT_D12: {                       \
+            typedef double R;                 \
+            constexpr int NE = 6;             \
+            __VA_ARGS__;                      \
+        } break;                              \
+        case FMT_F18: {                       \
+            typedef float R;                  \
+            constexpr int NE = 9;             \
+            __VA_ARGS__;                      \
+        } break;                              \
+        default: {                            \
+            typedef float R;                  \
+            constexpr int NE = 6;             \
+            __VA_ARGS__;                      \
+        } break;                              \
+    }
+#define DISPATCH_MU(mu, ...)       \
+    switch (mu) {                  \
+        case 0: {                  \
+            constexpr int MU = 0;  \
+            __VA_ARGS__;           \
+        } break;                   \
+        case 1: {                  \
+            constexpr int MU = 1;  \
+            __VA_ARGS__;           \
+        } break;                   \
+        case 2: {                  \
+            constexpr int MU = 2;  \
+            __VA_ARGS__;           \
+        } break;                   \
+        default: {                 \
+            constexpr int MU = 3;  \
+            __VA_ARGS__;           \
+        } break;                   \
+    }
+
+namespace {
+
+template <typename R, int NE>
+LinkField<R, NE> view(void* p, int64_t Vh) {
+    LinkField<R, NE> f;
+    f.p = (typename LinkField<R, NE>::C2*)p;
+    f.Vh = Vh;
+    return f;
+}
+template <typename R>
+AlgField<R> alg_view(void* p, int64_t Vh) {
+    AlgField<R> a;
+    a.p = (typename AlgField<R>::C2*)p;
+    a.Vh = Vh;
+    return a;
+}
+
+inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+// Grid size of the grid-stride reduction kernels: bounded so that the partial vectors
+// stay small, a multiple of the 148 SMs of a B200.
+inline unsigned red_blocks(int64_t n, int threads) {
+    unsigned b = blocks_for(n, threads);
+    return b < 148u * 8u ? b : 148u * 8u;
+}
+
+cudaEvent_t get_event(qcb_field_s* f) {
+    if (!f->event_pool.empty()) {
+        cudaEvent_t e = f->event_pool.back();
+        f->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Launch wrapper: launch counting, error check and optional event timing on the stream.
+template <class Fn>
+int launch(qcb_field_s* f, int kclass, Fn&& fn) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (f->timing) {
+        a = get_event(f);
+        b = get_event(f);
+        CK(cudaEventRecord(a, f->stream));
+    }
+    fn();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(QCB_ECUDA, "kernel launch: %s", cudaGetErrorString(e));
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (f->timing) {
+        CK(cudaEventRecord(b, f->stream));
+        f->pending.push_back(TimedLaunch{kclass, a, b});
+    }
+    return QCB_OK;
+}
+
+int ensure_partials(qcb_field_s* f, size_t n) {
+    if (f->partials_cap >= n) return QCB_OK;
+    if (f->partials) cudaFree(f->partials);
+    f->partials = nullptr;
+    f->partials_cap = 0;
+    CK(cudaMalloc(&f->partials, n * sizeof(double)));
+    f->partials_cap = n;
+    return QCB_OK;
+}
+int ensure_staging(qcb_field_s* f) {
+    if (f->staging) return QCB_OK;
+    CK(cudaMalloc(&f->staging, (size_t)f->g.V * 36 * sizeof(double2)));
+    return QCB_OK;
+}
+int ensure_alt(qcb_field_s* f) {
+    if (f->alt) return QCB_OK;
+    CK(cudaMalloc(&f->alt, link_bytes(f->fmt, f->g.Vh)));
+    return QCB_OK;
+}
+
+int check_err_flag(qcb_field_s* f) {
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, f->d_err, sizeof(int), cudaMemcpyDeviceToHost, f->stream));
+    CK(cudaStreamSynchronize(f->stream));
+    if (h & DERR_KP_CAP) {
+        CK(cudaMemsetAsync(f->d_err, 0, sizeof(int), f->stream));
+        return fail(QCB_ERANGE, "heatbath: Kennedy-Pendleton attempt cap reached");
+    }
+    return QCB_OK;
+}
+
+// reduction of nb partial vectors of nv doubles into dst (device)
+int finalize(qcb_field_s* f, int nb, int nv, unsigned max_mask, double* dst) {
+    return launch(f, QCB_K_OTHER, [&] { k_finalize<<<1, 256, 0, f->stream>>>(f->partials, nb, nv, max_mask, dst); });
+}
+
+// --- enqueue helpers (no host synchronisation) --------------------------------------
+int enq_plaquette(qcb_field_s* f, double* dst) {
+    const unsigned nbx = red_blocks(f->g.Vh, 256);
+    RET(ensure_partials(f, (size_t)nbx * 2));
+    int r = QCB_OK;
+    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_PLAQ, [&] {
+                     k_plaquette<R, NE><<<dim3(nbx, 2), 256, 0, f->stream>>>(f->g, view<R, NE>(f->links, f->g.Vh),
+                                                                                f->partials);
+                 }));
+    RET(r);
+    return finalize(f, (int)(nbx * 2), 1, 0u, dst);
+}
+int enq_clover(qcb_field_s* f, double* dst) {
+    const unsigned nbx = red_blocks(f->g.Vh, 128);
+    RET(ensure_partials(f, (size_t)nbx * 6 * 2));
+    int r = QCB_OK;
+    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_CLOVER, [&] {
+                     k_clover_qe<R, NE><<<dim3(nbx, 6), 128, 0, f->stream>>>(f->g, view<R, NE>(f->links, f->g.Vh),
+                                                                                f->partials);
+                 }));
+    RET(r);
+    return finalize(f, (int)(nbx * 6), 2, 0u, dst);
+}
+
+int read_results(qcb_field_s* f, int n) {
+    CK(cudaMemcpyAsync(f->h_res, f->d_res, n * sizeof(double), cudaMemcpyDeviceToHost, f->stream));
+    CK(cudaStreamSynchronize(f->stream));
+    return QCB_OK;
+}
+
+int upload_from_staging(qcb_field_s* f, int bswap) {
+    int r = QCB_OK;
+    const unsigned nb = blocks_for(f->g.V * 4, 256);
+    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
+                     k_aos_to_soa<R, NE><<<nb, 256, 0, f->stream>>>(f->g, f->staging, view<R, NE>(f->links, f->g.Vh),
+                                                                    bswap);
+                 }));
+    return r;
+}
+int download_to_staging(qcb_field_s* f, int bswap) {
+    int r = QCB_OK;
+    const unsigned nb = blocks_for(f->g.V * 4, 256);
+    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
+                     k_soa_to_aos<R, NE><<<nb, 256, 0, f->stream>>>(f->g, view<R, NE>(f->links, f->g.Vh), f->staging,
+                                                                    bswap);
+                 }));
+    return r;
+}
+
+int flow_stage(qcb_flow_s* fl, int stage) {
+    qcb_field_s* f = fl->fld;
+    RET(ensure_alt(f));
+    const unsigned nb = 8u * blocks_for(f->g.Vh, 128);
+    const int rep = (f->prec == QCB_PREC_F32) ? 1 : 0;
+    int r = QCB_OK;
+    DISPATCH_FMT(
+        f->fmt, r = launch(f, QCB_K_FLOW, [&] {
+            auto win = view<R, NE>(f->links, f->g.Vh);
+            auto wout = view<R, NE>(f->alt, f->g.Vh);
+            auto z = alg_view<R>(fl->z, f->g.Vh);
+            if (stage == 1)
+                k_flow_stage<R, NE, 1><<<nb, 128, 0, f->stream>>>(f->g, win, wout, z, fl->eps, rep);
+            else if (stage == 2)
+                k_flow_stage<R, NE, 2><<<nb, 128, 0, f->stream>>>(f->g, win, wout, z, fl->eps, rep);
+            else
+                k_flow_stage<R, NE, 3><<<nb, 128, 0, f->stream>>>(f->g, win, wout, z, fl->eps, rep);
+        }));
+    RET(r);
+    void* t = f->links;
+    f->links = f->alt;
+    f->alt = t;
+    return QCB_OK;
+}
+
+bool valid_L(const int L[4]) {
+    if (!L) return false;
+    int64_t V = 1;
+    for (int d = 0; d < 4; d++) {
+        if (L[d] < 2 || (L[d] & 1)) return false;
+        V *= L[d];
+    }
+    return V <= ((int64_t)1 << 30);
+}
+
+int field_new(const int L[4], int prec, int store, cudaStream_t stream, qcb_field_s** out) {
+    if (!out) return fail(QCB_EINVAL, "null output handle");
+    if (!valid_L(L)) return fail(QCB_EINVAL, "lattice extents must be even, >= 2, volume <= 2^30");
+    if (prec != QCB_PREC_F64 && prec != QCB_PREC_F32) return fail(QCB_EINVAL, "prec must be 64 or 32");
+    if (store != QCB_STORE_18 && store != QCB_STORE_12) return fail(QCB_EINVAL, "store must be 0 (18) or 1 (12)");
+    qcb_field_s* f = new (std::nothrow) qcb_field_s();
+    if (!f) return fail(QCB_ENOMEM, "host allocation");
+    for (int d = 0; d < 4; d++) f->L[d] = L[d];
+    f->g = make_geom(L);
+    f->prec = prec;
+    f->store = store;
+    f->fmt = fmt_of(prec, store);
+    cudaGetDevice(&f->device);
+    int r = QCB_OK;
+    cudaError_t e;
+    if (stream) {
+        f->stream = stream;
+    } else {
+        e = cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete f;
+            return fail(QCB_ECUDA, "stream: %s", cudaGetErrorString(e));
+        }
+        f->own_stream = true;
+    }
+    e = cudaMalloc(&f->links, link_bytes(f->fmt, f->g.Vh));
+    if (e == cudaSuccess) e = cudaMalloc(&f->d_res, 64 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&f->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&f->h_res, 64 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemsetAsync(f->d_err, 0, sizeof(int), f->stream);
+    if (e != cudaSuccess) {
+        r = fail(e == cudaErrorMemoryAllocation ? QCB_ENOMEM : QCB_ECUDA, "field allocation: %s",
+                 cudaGetErrorString(e));
+        qcb_field_destroy(f);
+        return r;
+    }
+    *out = f;
+    return qcb_cold_start(f);
+}
+
+}  // namespace
+
+// Deterministic final reduction (one block, fixed summation order for a given nb).
+__global__ void qcb::k_finalize(const double* partials, int nb, int nv, unsigned max_mask, double* out) {
+    __shared__ double sm[256];
+    for (int k = 0; k < nv; k++) {
+        const bool ismax = (max_mask >> k) & 1u;
+        double acc = 0.0;
+        for (int i = threadIdx.x; i < nb; i += 256) {
+            double v = partials[(size_t)i * nv + k];
+            acc = ismax ? fmax(acc, v) : acc + v;
+        }
+        sm[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = 128; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s) sm[threadIdx.x] = ismax ? fmax(sm[threadIdx.x], sm[threadIdx.x + s])
+                                                              : sm[threadIdx.x] + sm[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[k] = sm[0];
+        __syncthreads();
+    }
+}
+
+namespace {
+__global__ void k_diag_exp(const double2* Z, int n, double coeff, int f32, double2* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    M3<double> z;
+    for (int e = 0; e < 9; e++) z.e[e] = mkc(Z[i * 9 + e].x, Z[i * 9 + e].y);
+    for (int e = 0; e < 9; e++) z.e[e] = scl(coeff, z.e[e]);
+    M3<double> r;
+    if (f32) {
+        r = convert<double>(exp_su3(convert<float>(z)));
+    } else {
+        r = exp_su3(z);
+    }
+    for (int e = 0; e < 9; e++) out[i * 9 + e] = make_double2(r.e[e].re, r.e[e].im);
+}
+__global__ void k_diag_philox(uint4 ctr, uint2 key, int n, uint4* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t c[4] = {ctr.x + (uint32_t)i, ctr.y, ctr.z, ctr.w};
+    philox4x32_10(c, key.x, key.y);
+    out[i] = make_uint4(c[0], c[1], c[2], c[3]);
+}
+}  // namespace
+
+int qcb::field_upload_host(qcb_field_s* f, const double* host, int bswap) {
+    RET(ensure_staging(f));
+    CK(cudaMemcpyAsync(f->staging, host, (size_t)f->g.V * 36 * sizeof(double2), cudaMemcpyHostToDevice, f->stream));
+    RET(upload_from_staging(f, bswap));
+    CK(cudaStreamSynchronize(f->stream));
+    return QCB_OK;
+}
+int qcb::field_download_host(qcb_field_s* f, double* host, int bswap) {
+    RET(ensure_staging(f));
+    RET(download_to_staging(f, bswap));
+    CK(cudaMemcpyAsync(host, f->staging, (size_t)f->g.V * 36 * sizeof(double2), cudaMemcpyDeviceToHost, f->stream));
+    CK(cudaStreamSynchronize(f->stream));
+    return QCB_OK;
+}
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char* qcb_last_error(void) { return g_err.c_str(); }
+const char* qcb_version(void) { return "qcb 0.1 (sm_100a)"; }
+uint64_t qcb_launch_count(void) { return g_launches.load(); }
+
+int qcb_field_create(const int L[4], int prec, int store, qcb_field* out) {
+    return field_new(L, prec, store, nullptr, out);
+}
+
+int qcb_field_destroy(qcb_field f) {
+    if (!f) return QCB_OK;
+    if (f->stream) cudaStreamSynchronize(f->stream);
+    for (auto& t : f->pending) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    for (auto e : f->event_pool) cudaEventDestroy(e);
+    if (f->links) cudaFree(f->links);
+    if (f->alt) cudaFree(f->alt);
+    if (f->staging) cudaFree(f->staging);
+    if (f->partials) cudaFree(f->partials);
+    if (f->d_res) cudaFree(f->d_res);
+    if (f->d_err) cudaFree(f->d_err);
+    if (f->h_res) cudaFreeHost(f->h_res);
+    if (f->own_stream && f->stream) cudaStreamDestroy(f->stream);
+    delete f;
+    return QCB_OK;
+}
+
+int qcb_field_info(qcb_field f, int L[4], int* prec, int* store, size_t* device_bytes) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    if (L)
+        for (int d = 0; d < 4; d++) L[d] = f->L[d];
+    if (prec) *prec = f->prec;
+    if (store) *store = f->store;
+    if (device_bytes) *device_bytes = link_bytes(f->fmt, f->g.Vh);
+    return QCB_OK;
+}
+
+void* qcb_field_stream(qcb_field f) { return f ? (void*)f->stream : nullptr; }
+
+int qcb_field_set_stream(qcb_field f, void* s) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    CK(cudaStreamSynchronize(f->stream));
+    if (f->own_stream) cudaStreamDestroy(f->stream);
+    f->own_stream = false;
+    f->stream = (cudaStream_t)s;
+    return QCB_OK;
+}
+
+int qcb_field_sync(qcb_field f) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    CK(cudaStreamSynchronize(f->stream));
+    return QCB_OK;
+}
+
+int qcb_field_upload_aos(qcb_field f, const double* links) {
+    if (!f || !links) return fail(QCB_EINVAL, "null argument");
+    return field_upload_host(f, links, 0);
+}
+int qcb_field_download_aos(qcb_field f, double* links) {
+    if (!f || !links) return fail(QCB_EINVAL, "null argument");
+    return field_download_host(f, links, 0);
+}
+int qcb_field_upload_aos_device(qcb_field f, const double* d_links) {
+    if (!f || !d_links) return fail(QCB_EINVAL, "null argument");
+    int r = QCB_OK;
+    const unsigned nb = blocks_for(f->g.V * 4, 256);
+    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
+                     k_aos_to_soa<R, NE><<<nb, 256, 0, f->stream>>>(f->g, (const double2*)d_links,
+                                                                    view<R, NE>(f->links, f->g.Vh), 0);
+                 }));
+    return r;
+}
+int qcb_field_download_aos_device(qcb_field f, double* d_links) {
+    if (!f || !d_links) return fail(QCB_EINVAL, "null argument");
+    int r = QCB_OK;
+    const unsigned nb = blocks_for(f->g.V * 4, 256);
+    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
+                     k_soa_to_aos<R, NE><<<nb, 256, 0, f->stream>>>(f->g, view<R, NE>(f->links, f->g.Vh),
+                                                                    (double2*)d_links, 0);
+                 }));
+    return r;
+}
+
+int qcb_field_copy(qcb_field dst, qcb_field src) {
+    if (!dst || !src) return fail(QCB_EINVAL, "null field");
+    for (int d = 0; d < 4; d++)
+        if (dst->L[d] != src->L[d]) return fail(QCB_EINVAL, "copy between different lattices");
+    if (dst == src) return QCB_OK;
+    if (dst->stream != src->stream) {
+        cudaEvent_t ev;
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(ev, src->stream));
+        CK(cudaStreamWaitEvent(dst->stream, ev, 0));
+        cudaEventDestroy(ev);
+    }
+    if (dst->fmt == src->fmt) {
+        CK(cudaMemcpyAsync(dst->links, src->links, link_bytes(dst->fmt, dst->g.Vh), cudaMemcpyDeviceToDevice,
+                           dst->stream));
+        return QCB_OK;
+    }
+    RET(ensure_staging(dst));
+    int r = QCB_OK;
+    const unsigned nb = blocks_for(dst->g.V * 4, 256);
+    DISPATCH_FMT(src->fmt, r = launch(dst, QCB_K_OTHER, [&] {
+                     k_soa_to_aos<R, NE><<<nb, 256, 0, dst->stream>>>(src->g, view<R, NE>(src->links, src->g.Vh),
+                                                                      dst->staging, 0);
+                 }));
+    RET(r);
+    return upload_from_staging(dst, 0);
+}
+
+int qcb_cold_start(qcb_field f) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    int r = QCB_OK;
+    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
+                     k_start<R, NE><<<dim3(blocks_for(f->g.Vh, 128), 8), 128, 0, f->stream>>>(
+                         f->g, view<R, NE>(f->links, f->g.Vh), 0, 0ull);
+                 }));
+    return r;
+}
+
+int qcb_hot_start(qcb_field f, uint64_t seed) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    int r = QCB_OK;
+    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
+                     k_start<R, NE><<<dim3(blocks_for(f->g.Vh, 128), 8), 128, 0, f->stream>>>(
+                         f->g, view<R, NE>(f->links, f->g.Vh), 1, seed);
+                 }));
+    return r;
+}
+
+int qcb_reunitarize(qcb_field f) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    int r = QCB_OK;
+    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
+                     k_reunitarize<R, NE><<<dim3(blocks_for(f->g.Vh, 128), 8), 128, 0, f->stream>>>(
+                         f->g, view<R, NE>(f->links, f->g.Vh));
+                 }));
+    return r;
+}
+
+int qcb_unitarity(qcb_field f, double* max_err, double* mean_err) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    const unsigned nbx = red_blocks(f->g.Vh, 256);
+    RET(ensure_partials(f, (size_t)nbx * 8 * 2));
+    int r = QCB_OK;
+    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
+                     k_unitarity<R, NE><<<dim3(nbx, 8), 256, 0, f->stream>>>(f->g, view<R, NE>(f->links, f->g.Vh),
+                                                                                f->partials);
+                 }));
+    RET(r);
+    RET(finalize(f, (int)(nbx * 8), 2, 1u, f->d_res));
+    RET(read_results(f, 2));
+    if (max_err) *max_err = f->h_res[0];
+    if (mean_err) *mean_err = f->h_res[1] / (4.0 * (double)f->g.V);
+    return QCB_OK;
+}
+
+int qcb_shift(qcb_field f, const int s[4]) {
+    if (!f || !s) return fail(QCB_EINVAL, "null argument");
+    int sm[4];
+    bool any = false;
+    for (int d = 0; d < 4; d++) {
+        sm[d] = ((s[d] % f->L[d]) + f->L[d]) % f->L[d];
+        any = any || sm[d] != 0;
+    }
+    if (!any) return QCB_OK;
+    RET(ensure_alt(f));
+    int r = QCB_OK;
+    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
+                     k_shift<R, NE><<<dim3(blocks_for(f->g.Vh, 128), 8), 128, 0, f->stream>>>(
+                         f->g, view<R, NE>(f->links, f->g.Vh), view<R, NE>(f->alt, f->g.Vh), sm[0], sm[1], sm[2],
+                         sm[3]);
+                 }));
+    RET(r);
+    void* t = f->links;
+    f->links = f->alt;
+    f->alt = t;
+    return QCB_OK;
+}
+
+int qcb_random_shift(qcb_field f, uint64_t seed, uint64_t idx, int max_shift, int s_out[4]) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    uint32_t c[4] = {0u, (uint32_t)idx, (uint32_t)(idx >> 32), TAG_SHIFT};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    int s[4];
+    for (int d = 0; d < 4; d++) {
+        uint32_t n = (uint32_t)(max_shift > 0 ? max_shift : f->L[d]);
+        s[d] = (int)(((uint64_t)c[d] * n) >> 32);
+        if (s_out) s_out[d] = s[d];
+    }
+    return qcb_shift(f, s);
+}
+
+int qcb_hb_subsweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_t sweep, int parity, int mu) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    if (parity < 0 || parity > 1 || mu < 0 || mu > 3 || n_hits < 0 || !(beta > 0.0))
+        return fail(QCB_EINVAL, "heatbath: parity in {0,1}, mu in 0..3, n_hits >= 0, beta > 0");
+    const unsigned nb = blocks_for(f->g.Vh, 128);
+    const int rep = (f->prec == QCB_PREC_F32) ? 1 : 0;
+    int r = QCB_OK;
+    DISPATCH_FMT(f->fmt, DISPATCH_MU(mu, r = launch(f, QCB_K_HB, [&] {
+                                          k_hb_subsweep<R, NE, MU><<<nb, 128, 0, f->stream>>>(
+                                              f->g, view<R, NE>(f->links, f->g.Vh), parity, beta, n_hits, seed,
+                                              sweep, rep, f->d_err);
+                                      })));
+    return r;
+}
+
+int qcb_hb_sweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_t sweep) {
+    for (int p = 0; p < 2; p++)
+        for (int mu = 0; mu < 4; mu++) RET(qcb_hb_subsweep(f, beta, n_hits, seed, sweep, p, mu));
+    return QCB_OK;
+}
+
+int qcb_plaquette(qcb_field f, double* plaq) {
+    if (!f || !plaq) return fail(QCB_EINVAL, "null argument");
+    RET(enq_plaquette(f, f->d_res));
+    RET(read_results(f, 1));
+    *plaq = f->h_res[0] / (6.0 * (double)f->g.V);
+    return check_err_flag(f);
+}
+
+int qcb_clover_qe(qcb_field f, double* Q, double* E) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    RET(enq_clover(f, f->d_res));
+    RET(read_results(f, 2));
+    if (Q) *Q = f->h_res[0];
+    if (E) *E = f->h_res[1] / (double)f->g.V;
+    return QCB_OK;
+}
+
+// ------------------------------------------------------------------ flow
+int qcb_flow_create(qcb_field src, double eps, int prec, int store, qcb_flow* out) {
+    if (!src || !out) return fail(QCB_EINVAL, "null argument");
+    if (!(eps > 0.0)) return fail(QCB_EINVAL, "flow step must be > 0");
+    qcb_flow_s* fl = new (std::nothrow) qcb_flow_s();
+    if (!fl) return fail(QCB_ENOMEM, "host allocation");
+    fl->eps = eps;
+    int r = field_new(src->L, prec, store, src->stream, &fl->fld);
+    if (r != QCB_OK) {
+        delete fl;
+        return r;
+    }
+    cudaError_t e = cudaMalloc(&fl->z, alg_bytes(fl->fld->fmt, fl->fld->g.Vh));
+    if (e == cudaSuccess) e = cudaMalloc(&fl->fld->alt, link_bytes(fl->fld->fmt, fl->fld->g.Vh));
+    if (e != cudaSuccess) {
+        r = fail(e == cudaErrorMemoryAllocation ? QCB_ENOMEM : QCB_ECUDA, "flow allocation: %s",
+                 cudaGetErrorString(e));
+        qcb_flow_destroy(fl);
+        return r;
+    }
+    r = qcb_field_copy(fl->fld, src);
+    if (r != QCB_OK) {
+        qcb_flow_destroy(fl);
+        return r;
+    }
+    *out = fl;
+    return QCB_OK;
+}
+
+int qcb_flow_destroy(qcb_flow fl) {
+    if (!fl) return QCB_OK;
+    if (fl->fld && fl->fld->stream) cudaStreamSynchronize(fl->fld->stream);
+    if (fl->z) cudaFree(fl->z);
+    qcb_field_destroy(fl->fld);
+    delete fl;
+    return QCB_OK;
+}
+
+int qcb_flow_copy(qcb_flow fl, qcb_field src) {
+    if (!fl || !src) return fail(QCB_EINVAL, "null argument");
+    return qcb_field_copy(fl->fld, src);
+}
+
+int qcb_flow_rk3(qcb_flow fl, int n) {
+    if (!fl || n < 0) return fail(QCB_EINVAL, "invalid argument");
+    for (int i = 0; i < n; i++) {
+        RET(flow_stage(fl, 1));
+        RET(flow_stage(fl, 2));
+        RET(flow_stage(fl, 3));
+    }
+    return QCB_OK;
+}
+
+int qcb_flow_measure(qcb_flow fl, qcb_field src, int n_steps, int n_rk, double* tQE, double* plaq) {
+    if (!fl || !src || !tQE || n_steps < 1 || n_rk < 0) return fail(QCB_EINVAL, "invalid argument");
+    qcb_field_s* f = fl->fld;
+    RET(qcb_field_copy(f, src));
+    double* d_meas = nullptr;
+    CK(cudaMallocAsync((void**)&d_meas, (size_t)n_steps * 3 * sizeof(double), f->stream));
+    int r = QCB_OK;
+    for (int s = 0; s < n_steps && r == QCB_OK; s++) {
+        r = enq_clover(f, d_meas + 3 * s);
+        if (r == QCB_OK && plaq) r = enq_plaquette(f, d_meas + 3 * s + 2);
+        if (r == QCB_OK && s != n_steps - 1) r = qcb_flow_rk3(fl, n_rk);
+    }
+    std::vector<double> h((size_t)n_steps * 3);
+    if (r == QCB_OK) {
+        cudaError_t e = cudaMemcpyAsync(h.data(), d_meas, h.size() * sizeof(double), cudaMemcpyDeviceToHost, f->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
+        if (e != cudaSuccess) r = fail(QCB_ECUDA, "flow measure readback: %s", cudaGetErrorString(e));
+    }
+    cudaFreeAsync(d_meas, f->stream);
+    RET(r);
+    double t = 0.0;
+    for (int s = 0; s < n_steps; s++) {
+        tQE[3 * s] = t;
+        tQE[3 * s + 1] = h[3 * s];
+        tQE[3 * s + 2] = h[3 * s + 1] / (double)f->g.V;
+        if (plaq) plaq[s] = h[3 * s + 2] / (6.0 * (double)f->g.V);
+        if (s != n_steps - 1)
+            for (int k = 0; k < n_rk; k++) t += fl->eps;
+    }
+    return QCB_OK;
+}
+
+qcb_field qcb_flow_field(qcb_flow fl) { return fl ? fl->fld : nullptr; }
+
+// ------------------------------------------------------------------ instrumentation
+int qcb_timing_enable(qcb_field f, int on) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    f->timing = on != 0;
+    return QCB_OK;
+}
+
+int qcb_timing_read(qcb_field f, int kclass, long* launches, double* total_ms) {
+    if (!f || kclass < 0 || kclass >= QCB_K_NCLASS) return fail(QCB_EINVAL, "invalid argument");
+    CK(cudaStreamSynchronize(f->stream));
+    for (auto& t : f->pending) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, t.a, t.b));
+        f->t_count[t.kclass] += 1;
+        f->t_ms[t.kclass] += ms;
+        f->event_pool.push_back(t.a);
+        f->event_pool.push_back(t.b);
+    }
+    f->pending.clear();
+    if (launches) *launches = f->t_count[kclass];
+    if (total_ms) *total_ms = f->t_ms[kclass];
+    return QCB_OK;
+}
+
+int qcb_timing_reset(qcb_field f) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    long n;
+    double ms;
+    RET(qcb_timing_read(f, 0, &n, &ms));
+    for (int k = 0; k < QCB_K_NCLASS; k++) {
+        f->t_count[k] = 0;
+        f->t_ms[k] = 0.0;
+    }
+    return QCB_OK;
+}
+
+// ------------------------------------------------------------------ diagnostics
+int qcb_diag_staple(qcb_field f, int mu, double* out) {
+    if (!f || !out || mu < 0 || mu > 3) return fail(QCB_EINVAL, "invalid argument");
+    RET(ensure_staging(f));
+    int r = QCB_OK;
+    DISPATCH_FMT(f->fmt, DISPATCH_MU(mu, r = launch(f, QCB_K_OTHER, [&] {
+                                          k_staple_field<R, NE, MU><<<dim3(blocks_for(f->g.Vh, 128), 2), 128, 0,
+                                                                      f->stream>>>(
+                                              f->g, view<R, NE>(f->links, f->g.Vh), f->staging);
+                                      })));
+    RET(r);
+    CK(cudaMemcpyAsync(out, f->staging, (size_t)f->g.V * 9 * sizeof(double2), cudaMemcpyDeviceToHost, f->stream));
+    CK(cudaStreamSynchronize(f->stream));
+    return QCB_OK;
+}
+
+int qcb_diag_exp_su3(const double* Z, int n, double coeff, int prec, double* out) {
+    if (!Z || !out || n < 0) return fail(QCB_EINVAL, "invalid argument");
+    if (n == 0) return QCB_OK;
+    double2 *dz = nullptr, *dout = nullptr;
+    size_t bytes = (size_t)n * 9 * sizeof(double2);
+    CK(cudaMalloc(&dz, bytes));
+    cudaError_t e = cudaMalloc(&dout, bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(dz, Z, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_diag_exp<<<(n + 127) / 128, 128>>>(dz, n, coeff, prec == QCB_PREC_F32 ? 1 : 0, dout);
+        g_launches.fetch_add(1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(dz);
+    cudaFree(dout);
+    if (e != cudaSuccess) return fail(QCB_ECUDA, "diag exp: %s", cudaGetErrorString(e));
+    return QCB_OK;
+}
+
+int qcb_diag_philox(const uint32_t ctr[4], const uint32_t key[2], int n, uint32_t* out) {
+    if (!ctr || !key || !out || n < 0) return fail(QCB_EINVAL, "invalid argument");
+    if (n == 0) return QCB_OK;
+    uint4* d = nullptr;
+    CK(cudaMalloc(&d, (size_t)n * sizeof(uint4)));
+    k_diag_philox<<<(n + 127) / 128, 128>>>(make_uint4(ctr[0], ctr[1], ctr[2], ctr[3]), make_uint2(key[0], key[1]), n,
+                                           d);
+    g_launches.fetch_add(1);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, (size_t)n * sizeof(uint4), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(QCB_ECUDA, "diag philox: %s", cudaGetErrorString(e));
+    return QCB_OK;
+}
+
+}  // extern "C"

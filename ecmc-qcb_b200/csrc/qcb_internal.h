@@ -1,0 +1,64 @@
+// qcb_internal.h -- host-side internals shared by the C ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdarg.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/qcb.h"
+#include "qcb_field.cuh"
+
+namespace qcb {
+
+// Storage format of a field: index into {D18, D12, F18, F12}.
+enum Fmt : int { FMT_D18 = 0, FMT_D12 = 1, FMT_F18 = 2, FMT_F12 = 3 };
+inline int fmt_of(int prec, int store) { return (prec == QCB_PREC_F32 ? 2 : 0) + (store == QCB_STORE_12 ? 1 : 0); }
+inline int fmt_ne(int fmt) { return (fmt & 1) ? 6 : 9; }
+inline size_t fmt_cbytes(int fmt) { return (fmt & 2) ? sizeof(float2) : sizeof(double2); }
+inline size_t link_bytes(int fmt, int64_t Vh) { return (size_t)8 * fmt_ne(fmt) * (size_t)Vh * fmt_cbytes(fmt); }
+inline size_t alg_bytes(int fmt, int64_t Vh) { return (size_t)8 * 4 * (size_t)Vh * fmt_cbytes(fmt); }
+
+int fail(int code, const char* fmt, ...);
+
+struct TimedLaunch {
+    int kclass;
+    cudaEvent_t a, b;
+};
+
+}  // namespace qcb
+
+struct qcb_field_s {
+    int L[4];
+    qcb::Geom g;
+    int prec, store, fmt;
+    int device;
+    void* links = nullptr;  // current link buffer
+    void* alt = nullptr;    // second link buffer (shift target), lazily allocated
+    double2* staging = nullptr;  // device AoS staging buffer, lazily allocated
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    double* partials = nullptr;
+    size_t partials_cap = 0;  // doubles
+    double* d_res = nullptr;  // device results (8 doubles)
+    double* h_res = nullptr;  // pinned host results (8 doubles)
+    int* d_err = nullptr;     // device error flags
+    bool timing = false;
+    std::vector<qcb::TimedLaunch> pending;
+    std::vector<cudaEvent_t> event_pool;
+    long t_count[QCB_K_NCLASS] = {0};
+    double t_ms[QCB_K_NCLASS] = {0};
+};
+
+struct qcb_flow_s {
+    qcb_field_s* fld = nullptr;  // flowed field (owned); fld->links holds W
+    void* wtmp = nullptr;         // ping-pong partner of fld->links
+    void* z = nullptr;            // su(3) accumulator, 8 reals per link
+    double eps = 0.02;
+};
+
+namespace qcb {
+// Raw AoS transfers used by the ILDG reader / writer.
+int field_upload_host(qcb_field_s* f, const double* host, int bswap);
+int field_download_host(qcb_field_s* f, double* host, int bswap);
+}  // namespace qcb

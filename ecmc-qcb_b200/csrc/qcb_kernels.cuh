@@ -1,0 +1,515 @@
+// qcb_kernels.cuh -- sm_100a kernels of the gauge-field hot path.
+//
+// Every kernel is templated on the storage real type R (double / float) and on the
+// number of stored complex entries per link NE (9 = 18 reals, 6 = 12 reals).
+#pragma once
+#include <stdint.h>
+
+#include "qcb_field.cuh"
+
+namespace qcb {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// Device error flags (bit mask written by kernels, read by the host after a sync).
+enum : int { DERR_KP_CAP = 1 };
+
+// byte reversal of a double (ILDG files are big-endian, src/io/ildg.cpp:25-32)
+__device__ __forceinline__ double bswap_f64(double x) {
+    unsigned long long v = (unsigned long long)__double_as_longlong(x);
+    unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
+    unsigned long long r = ((unsigned long long)__byte_perm(lo, 0u, 0x0123u) << 32) | __byte_perm(hi, 0u, 0x0123u);
+    return __longlong_as_double((long long)r);
+}
+
+// ------------------------------------------------------------------ staple
+// compute_staple (src/gauge/GaugeField.cpp:74-97):
+//   A = sum_{nu != mu} U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag + U_nu(x+mu-nu)^dag U_mu(x-nu)^dag U_nu(x-nu)
+// x has parity `par`; x+-nu and x+mu have parity 1-par; x+mu-nu has parity `par`.
+template <typename R, int NE, int MU, bool RO>
+__device__ __forceinline__ M3<R> staple(const Geom& g, const LinkField<R, NE>& U, const int c[4], int64_t lex,
+                                        int par) {
+    M3<R> A;
+    set_zero(A);
+    const int opp = par ^ 1;
+    const int64_t xmu = step_up(g, lex, c[MU], MU);
+#pragma unroll
+    for (int nu = 0; nu < 4; nu++) {
+        if (nu == MU) continue;
+        const int64_t xnu = step_up(g, lex, c[nu], nu);
+        const int64_t xmnu = step_dn(g, lex, c[nu], nu);
+        const int64_t xmumnu = step_dn(g, xmu, c[nu], nu);
+        {
+            M3<R> a = RO ? U.load_ro(nu, opp, xmu >> 1) : U.load(nu, opp, xmu >> 1);
+            M3<R> b = RO ? U.load_ro(MU, opp, xnu >> 1) : U.load(MU, opp, xnu >> 1);
+            M3<R> t = mul_na(a, b);
+            M3<R> d = RO ? U.load_ro(nu, par, lex >> 1) : U.load(nu, par, lex >> 1);
+            acc_na(A, t, d);
+        }
+        {
+            M3<R> v1 = RO ? U.load_ro(MU, opp, xmnu >> 1) : U.load(MU, opp, xmnu >> 1);
+            M3<R> v0 = RO ? U.load_ro(nu, par, xmumnu >> 1) : U.load(nu, par, xmumnu >> 1);
+            M3<R> t = mul_nn(v1, v0);
+            M3<R> v2 = RO ? U.load_ro(nu, opp, xmnu >> 1) : U.load(nu, opp, xmnu >> 1);
+            acc_an(A, t, v2);
+        }
+    }
+    return A;
+}
+
+// ------------------------------------------------------------------ heatbath
+struct Quat {
+    double a0, a1, a2, a3;
+};
+
+// generate_su2_kp (src/heatbath/heatbath.cpp:8-36) + su2_step (:39-44).
+// The Kennedy-Pendleton loop has an attempt cap (never reached for beta*k > 1e-3); on the
+// cap the link keeps r = identity and the kernel raises DERR_KP_CAP.
+__device__ __forceinline__ Quat su2_step(double beta, Quat w, LinkStream& rng, int* err) {
+    double k = sqrt(w.a0 * w.a0 + w.a1 * w.a1 + w.a2 * w.a2 + w.a3 * w.a3);
+    double ik = 1.0 / k;
+    Quat v = {w.a0 * ik, w.a1 * ik, w.a2 * ik, w.a3 * ik};
+    double alpha = beta * k * 2.0 / 3.0;
+    double m05a = -0.5 / alpha;
+    double a0 = 1.0;
+    bool ok = false;
+    for (int it = 0; it < (1 << 20); it++) {
+        double delta = rng.next();
+        double r1 = rng.next();
+        double r2 = rng.next();
+        double r3 = rng.next();
+        double c = cospi(2.0 * r2);
+        double lsq = __dmul_rn(m05a, __dadd_rn(log(r1), __dmul_rn(__dmul_rn(c, c), log(r3))));
+        if (__dmul_rn(delta, delta) <= __dadd_rn(1.0, -lsq)) {
+            a0 = __dadd_rn(1.0, -__dmul_rn(2.0, lsq));
+            ok = true;
+            break;
+        }
+    }
+    if (!ok) {
+        atomicOr(err, (int)DERR_KP_CAP);
+        return Quat{1.0, 0.0, 0.0, 0.0};
+    }
+    double rs = sqrt(1.0 - a0 * a0);
+    double uphi = rng.next();
+    double cos_t = 2.0 * rng.next() - 1.0;
+    double sin_t = sqrt(1.0 - cos_t * cos_t);
+    double sp, cp;
+    sincospi(2.0 * uphi, &sp, &cp);
+    Quat x = {a0, rs * sin_t * cp, rs * sin_t * sp, rs * cos_t};
+    // mult(x, adj(v))  (src/su3/utils.cpp:53-63)
+    Quat q = {x.a0 * v.a0 + x.a1 * v.a1 + x.a2 * v.a2 + x.a3 * v.a3,
+              -x.a0 * v.a1 + x.a1 * v.a0 - x.a2 * v.a3 + x.a3 * v.a2,
+              -x.a0 * v.a2 + x.a1 * v.a3 + x.a2 * v.a0 - x.a3 * v.a1,
+              -x.a0 * v.a3 - x.a1 * v.a2 + x.a2 * v.a1 + x.a3 * v.a0};
+    return q;
+}
+
+// One Cabibbo-Marinari subgroup update of u in place (src/heatbath/heatbath_mpi.cpp:14-32):
+// w = quaternion of the (I,J) block of W = u*A, r = su2_step(w), u <- embed_{IJ}(r) * u.
+template <typename R, int I, int J>
+__device__ __forceinline__ void cm_subgroup(M3<R>& u, const M3<R>& A, double beta, LinkStream& rng, int* err) {
+    Cx<R> wii = mkc<R>(0, 0), wij = mkc<R>(0, 0), wji = mkc<R>(0, 0), wjj = mkc<R>(0, 0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        cmac(wii, u(I, k), A(k, I));
+        cmac(wij, u(I, k), A(k, J));
+        cmac(wji, u(J, k), A(k, I));
+        cmac(wjj, u(J, k), A(k, J));
+    }
+    // su2_to_quaternion (src/su3/utils.cpp:47-50)
+    Quat w = {((double)wii.re + (double)wjj.re) / 2.0, ((double)wij.im + (double)wji.im) / 2.0,
+              ((double)wij.re - (double)wji.re) / 2.0, ((double)wii.im - (double)wjj.im) / 2.0};
+    Quat r = su2_step(beta, w, rng, err);
+    // su2_quaternion_to_su3 (src/su3/utils.cpp:33-44) applied from the left
+    Cx<R> rii = mkc<R>((R)r.a0, (R)r.a3), rjj = mkc<R>((R)r.a0, (R)-r.a3);
+    Cx<R> rij = mkc<R>((R)r.a2, (R)r.a1), rji = mkc<R>((R)-r.a2, (R)r.a1);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        Cx<R> ui = u(I, k), uj = u(J, k);
+        Cx<R> ni = rii * ui;
+        cmac(ni, rij, uj);
+        Cx<R> nj = rji * ui;
+        cmac(nj, rjj, uj);
+        u(I, k) = ni;
+        u(J, k) = nj;
+    }
+}
+
+// Heatbath update of every link (x, MU) with parity(x) == par (one (parity, direction)
+// set of the checkerboard: no link of the set appears in another's staple, so all of them
+// update concurrently).  Replaces mpi::heatbathcb::sweep (heatbath_mpi.cpp:36-57) for one
+// (parity, mu); the staple is computed once per link, since it does not contain U(x,MU)
+// and is therefore identical for every hit (the reference recomputes it per hit).
+template <typename R, int NE, int MU>
+__global__ void __launch_bounds__(128) k_hb_subsweep(Geom g, LinkField<R, NE> U, int par, double beta, int n_hits,
+                                                      uint64_t seed, uint32_t sweep, int reproject, int* err) {
+    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= g.Vh) return;
+    int c[4];
+    site_coords(g, par, (uint32_t)h, c);
+    const int64_t lex = lex_of(g, c);
+    M3<R> A = staple<R, NE, MU, true>(g, U, c, lex, par);
+    M3<R> u = U.load(MU, par, h);
+    LinkStream rng(seed, (uint32_t)(lex * 4 + MU), sweep, TAG_HB);
+    for (int hit = 0; hit < n_hits; hit++) {
+        cm_subgroup<R, 0, 1>(u, A, beta, rng, err);
+        cm_subgroup<R, 1, 2>(u, A, beta, rng, err);
+        cm_subgroup<R, 0, 2>(u, A, beta, rng, err);
+    }
+    if (reproject) {
+        M3<double> ud = convert<double>(u);
+        project_su3(ud);
+        u = convert<R>(ud);
+    }
+    U.store(MU, par, h, u);
+}
+
+// ------------------------------------------------------------------ Wilson flow
+// One fused RK3 stage (src/flow/gradient_flow.cpp:17-121) for every link (x, mu):
+//   F = proj_lie_su3(-U A)                                          compute_force
+//   stage 1: Z = F;               W' = exp(eps/4 * F) W             compute_w1
+//   stage 2: W' = exp(8/9 eps F - 17/36 eps Z) W;  Z = 8/9 F - 17/36 Z   compute_w2 + replace_force_0
+//   stage 3: W' = exp(3/4 eps F - eps Z) W                          compute_w3
+// The whole field of forces is never materialised: Win is read-only for the launch and W'
+// goes to a second buffer (ping-pong), which is what makes force and update one pass.
+template <typename R, int NE, int STAGE, int MU>
+__device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>& Win, const LinkField<R, NE>& Wout,
+                                          const AlgField<R>& Z, double eps, int par, int64_t h, int reproject) {
+    int c[4];
+    site_coords(g, par, (uint32_t)h, c);
+    const int64_t lex = lex_of(g, c);
+    M3<R> A = staple<R, NE, MU, true>(g, Win, c, lex, par);
+    M3<R> u = Win.load_ro(MU, par, h);
+    M3<R> F = proj_lie(mul_nn(u, A));
+#pragma unroll
+    for (int k = 0; k < 9; k++) F.e[k] = mkc<R>(-F.e[k].re, -F.e[k].im);  // proj_lie(-UA) = -proj_lie(UA)
+    M3<R> X;
+    if (STAGE == 1) {
+        const R c1 = (R)(0.25 * eps);
+#pragma unroll
+        for (int k = 0; k < 9; k++) X.e[k] = scl(c1, F.e[k]);
+        Z.store(MU, par, h, F);
+    } else if (STAGE == 2) {
+        M3<R> z0 = Z.load(MU, par, h);
+        const R a = (R)((8.0 / 9.0) * eps), b = (R)((17.0 / 36.0) * eps);
+        const R a1 = (R)(8.0 / 9.0), b1 = (R)(17.0 / 36.0);
+        M3<R> zn;
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            X.e[k] = scl(a, F.e[k]) - scl(b, z0.e[k]);
+            zn.e[k] = scl(a1, F.e[k]) - scl(b1, z0.e[k]);
+        }
+        Z.store(MU, par, h, zn);
+    } else {
+        M3<R> z0 = Z.load(MU, par, h);
+        const R a = (R)(0.75 * eps), b = (R)eps;
+#pragma unroll
+        for (int k = 0; k < 9; k++) X.e[k] = scl(a, F.e[k]) - scl(b, z0.e[k]);
+    }
+    M3<R> E = exp_su3(X);
+    M3<R> w = mul_nn(E, u);
+    if (reproject) {
+        M3<double> wd = convert<double>(w);
+        project_su3(wd);
+        w = convert<R>(wd);
+    }
+    Wout.store(MU, par, h, w);
+}
+
+// Grid: blockIdx.x = (site block) * 8 + (mu*2 + parity), so the 8 link classes of a block of
+// sites run together and share their neighbour links in L2.
+template <typename R, int NE, int STAGE>
+__global__ void __launch_bounds__(128) k_flow_stage(Geom g, LinkField<R, NE> Win, LinkField<R, NE> Wout,
+                                                     AlgField<R> Z, double eps, int reproject) {
+    const int lt = blockIdx.x & 7;
+    const int mu = lt >> 1, par = lt & 1;
+    const int64_t h = (int64_t)(blockIdx.x >> 3) * blockDim.x + threadIdx.x;
+    if (h >= g.Vh) return;
+    switch (mu) {
+        case 0: flow_link<R, NE, STAGE, 0>(g, Win, Wout, Z, eps, par, h, reproject); break;
+        case 1: flow_link<R, NE, STAGE, 1>(g, Win, Wout, Z, eps, par, h, reproject); break;
+        case 2: flow_link<R, NE, STAGE, 2>(g, Win, Wout, Z, eps, par, h, reproject); break;
+        default: flow_link<R, NE, STAGE, 3>(g, Win, Wout, Z, eps, par, h, reproject); break;
+    }
+}
+
+// ------------------------------------------------------------------ reductions
+// Block reduction of NV doubles -> partials[blockIdx * NV + k] (warp shuffles, then one
+// warp).  Component k is a maximum when bit k of MAXMASK is set, a sum otherwise.
+template <int NV, unsigned MAXMASK = 0u>
+__device__ __forceinline__ void block_sum_store(double v[NV], double* partials, int block_id) {
+    __shared__ double sm[32][NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            double o = __shfl_down_sync(0xffffffffu, v[k], off);
+            v[k] = ((MAXMASK >> k) & 1u) ? fmax(v[k], o) : v[k] + o;
+        }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; k++) sm[wid][k] = v[k];
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double s = lane < nw ? sm[lane][k] : 0.0;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                double o = __shfl_down_sync(0xffffffffu, s, off);
+                s = ((MAXMASK >> k) & 1u) ? fmax(s, o) : s + o;
+            }
+            if (lane == 0) partials[(size_t)block_id * NV + k] = s;
+        }
+    }
+}
+
+// Deterministic final sum of nb partial vectors (one block of 256 threads; fixed order).
+// mode bit k set: component k is a max instead of a sum.
+__global__ void k_finalize(const double* partials, int nb, int nv, unsigned max_mask, double* out);
+
+// Plaquette (observables_mpi.cpp:11-35): per site sum over mu<nu of Re Tr(U_mu(x) U_nu(x+mu)
+// U_mu(x+nu)^dag U_nu(x)^dag)/3, evaluated as Re Tr((U_mu(x) U_nu(x+mu)) (U_nu(x) U_mu(x+nu))^dag).
+template <typename R, int NE>
+__global__ void __launch_bounds__(256) k_plaquette(Geom g, LinkField<R, NE> U, double* partials) {
+    const int par = blockIdx.y;
+    double v[1] = {0.0};
+    for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.x * blockDim.x) {
+        int c[4];
+        site_coords(g, par, (uint32_t)h, c);
+        const int64_t lex = lex_of(g, c);
+        double s = 0.0;
+#pragma unroll
+        for (int mu = 0; mu < 4; mu++) {
+            const int64_t xmu = step_up(g, lex, c[mu], mu);
+            M3<R> umu = U.load_ro(mu, par, h);
+#pragma unroll
+            for (int nu = mu + 1; nu < 4; nu++) {
+                const int64_t xnu = step_up(g, lex, c[nu], nu);
+                M3<R> p1 = mul_nn(umu, U.load_ro(nu, par ^ 1, xmu >> 1));
+                M3<R> p2 = mul_nn(U.load_ro(nu, par, h), U.load_ro(mu, par ^ 1, xnu >> 1));
+                s += (double)re_tr_mul_na(p1, p2) / 3.0;
+            }
+        }
+        v[0] += s;
+    }
+    block_sum_store<1>(v, partials, blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// clover_site (observables_mpi.cpp:66-90): F = (C - C^dag)/8 with the four leaves in the
+// reference's order and association.
+template <typename R, int NE>
+__device__ __forceinline__ M3<R> clover_F(const Geom& g, const LinkField<R, NE>& U, const int c[4], int64_t lex,
+                                          int par, int mu, int nu) {
+    const int opp = par ^ 1;
+    const int64_t xpmu = step_up(g, lex, c[mu], mu), xpnu = step_up(g, lex, c[nu], nu);
+    const int64_t xmmu = step_dn(g, lex, c[mu], mu), xmnu = step_dn(g, lex, c[nu], nu);
+    const int64_t xmmupnu = step_up(g, xmmu, c[nu], nu), xmmumnu = step_dn(g, xmmu, c[nu], nu);
+    const int64_t xpmumnu = step_dn(g, xpmu, c[nu], nu);
+    const int64_t h = lex >> 1;
+    M3<R> C, t;
+    // leaf 1: U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
+    t = mul_nn(U.load_ro(mu, par, h), U.load_ro(nu, opp, xpmu >> 1));
+    t = mul_na(t, U.load_ro(mu, opp, xpnu >> 1));
+    C = mul_na(t, U.load_ro(nu, par, h));
+    // leaf 2: U_nu(x) U_mu(x-mu+nu)^dag U_nu(x-mu)^dag U_mu(x-mu)
+    t = mul_na(U.load_ro(nu, par, h), U.load_ro(mu, par, xmmupnu >> 1));
+    t = mul_na(t, U.load_ro(nu, opp, xmmu >> 1));
+    acc_nn(C, t, U.load_ro(mu, opp, xmmu >> 1));
+    // leaf 3: U_mu(x-mu)^dag U_nu(x-mu-nu)^dag U_mu(x-mu-nu) U_nu(x-nu)
+    t = mul_nn(U.load_ro(nu, par, xmmumnu >> 1), U.load_ro(mu, opp, xmmu >> 1));
+    t = mul_an(t, U.load_ro(mu, par, xmmumnu >> 1));
+    acc_nn(C, t, U.load_ro(nu, opp, xmnu >> 1));
+    // leaf 4: U_nu(x-nu)^dag U_mu(x-nu) U_nu(x+mu-nu) U_mu(x)^dag
+    t = mul_an(U.load_ro(nu, opp, xmnu >> 1), U.load_ro(mu, opp, xmnu >> 1));
+    t = mul_nn(t, U.load_ro(nu, par, xpmumnu >> 1));
+    acc_na(C, t, U.load_ro(mu, par, h));
+    M3<R> F;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) F(i, j) = scl((R)0.125, C(i, j) - cconj(C(j, i)));
+    return F;
+}
+
+// local_q_e_clover (observables_mpi.cpp:93-112), one thread per (site, plane pair):
+// pair 0: +Re Tr(F01 F23), pair 1: -Re Tr(F02 F13), pair 2: +Re Tr(F03 F12); e += |F|^2/2.
+template <typename R, int NE>
+__global__ void __launch_bounds__(128) k_clover_qe(Geom g, LinkField<R, NE> U, double* partials) {
+    const int par = blockIdx.y & 1, pair = blockIdx.y >> 1;
+    const int a_mu = 0, a_nu = pair + 1;
+    const int b_mu = (pair == 0) ? 2 : 1, b_nu = (pair == 2) ? 2 : 3;
+    double v[2] = {0.0, 0.0};
+    for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.x * blockDim.x) {
+        int c[4];
+        site_coords(g, par, (uint32_t)h, c);
+        const int64_t lex = lex_of(g, c);
+        M3<R> Fa = clover_F(g, U, c, lex, par, a_mu, a_nu);
+        M3<R> Fb = clover_F(g, U, c, lex, par, b_mu, b_nu);
+        double q = (double)re_tr_mul(Fa, Fb);
+        v[0] += (pair == 1 ? -q : q) * (1.0 / (4.0 * kPi * kPi));
+        v[1] += 0.5 * ((double)sq_norm(Fa) + (double)sq_norm(Fb));
+    }
+    block_sum_store<2>(v, partials, blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// Unitarity error ||U U^dag - 1||_F per link (src/bin/test.cpp:58-72): partials (max, sum).
+template <typename R, int NE>
+__global__ void __launch_bounds__(256) k_unitarity(Geom g, LinkField<R, NE> U, double* partials) {
+    const int lt = blockIdx.y;
+    const int mu = lt >> 1, par = lt & 1;
+    double v[2] = {0.0, 0.0};
+    for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.x * blockDim.x) {
+        M3<double> u = convert<double>(U.load_ro(mu, par, h));
+        M3<double> d = mul_na(u, u);
+        d(0, 0).re -= 1.0;
+        d(1, 1).re -= 1.0;
+        d(2, 2).re -= 1.0;
+        double err = sqrt(sq_norm(d));
+        v[0] = fmax(v[0], err);
+        v[1] += err;
+    }
+    block_sum_store<2, 1u>(v, partials, blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// ------------------------------------------------------------------ layout, starts, shift
+// AoS (site lex, mu, row-major 3x3 complex; optionally big-endian) -> parity-split SoA.
+template <typename R, int NE>
+__global__ void k_aos_to_soa(Geom g, const double2* aos, LinkField<R, NE> U, int bswap) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.V * 4) return;
+    const int64_t lex = t >> 2;
+    const int mu = (int)(t & 3);
+    int c[4];
+    lex_coords(g, lex, c);
+    const int par = (c[0] + c[1] + c[2] + c[3]) & 1;
+    M3<R> u;
+#pragma unroll
+    for (int e = 0; e < 9; e++) {
+        double2 v = aos[t * 9 + e];
+        if (bswap) {
+            v.x = bswap_f64(v.x);
+            v.y = bswap_f64(v.y);
+        }
+        u.e[e] = mkc<R>((R)v.x, (R)v.y);
+    }
+    U.store(mu, par, lex >> 1, u);
+}
+template <typename R, int NE>
+__global__ void k_soa_to_aos(Geom g, LinkField<R, NE> U, double2* aos, int bswap) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.V * 4) return;
+    const int64_t lex = t >> 2;
+    const int mu = (int)(t & 3);
+    int c[4];
+    lex_coords(g, lex, c);
+    const int par = (c[0] + c[1] + c[2] + c[3]) & 1;
+    M3<R> u = U.load_ro(mu, par, lex >> 1);
+#pragma unroll
+    for (int e = 0; e < 9; e++) {
+        double2 v;
+        v.x = (double)u.e[e].re;
+        v.y = (double)u.e[e].im;
+        if (bswap) {
+            v.x = bswap_f64(v.x);
+            v.y = bswap_f64(v.y);
+        }
+        aos[t * 9 + e] = v;
+    }
+}
+
+// cold_start (GaugeField.cpp:23-33) / hot_start (GaugeField.cpp:10-20) with a Haar SU(3)
+// generator: two complex Gaussian columns from the link's Philox stream (Box-Muller),
+// orthonormalised and completed by projection_su3 (GaugeField.cpp:36-58), in double.
+template <typename R, int NE>
+__global__ void k_start(Geom g, LinkField<R, NE> U, int hot, uint64_t seed) {
+    const int lt = blockIdx.y;
+    const int mu = lt >> 1, par = lt & 1;
+    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= g.Vh) return;
+    M3<double> m;
+    if (!hot) {
+        m = ident<double>();
+    } else {
+        int c[4];
+        site_coords(g, par, (uint32_t)h, c);
+        const int64_t lex = lex_of(g, c);
+        LinkStream rng(seed, (uint32_t)(lex * 4 + mu), 0u, TAG_HOT);
+        double gs[12];
+#pragma unroll
+        for (int k = 0; k < 12; k += 2) {
+            double u1 = rng.next(), u2 = rng.next();
+            double r = sqrt(-2.0 * log(1.0 - u1));
+            double s, co;
+            sincospi(2.0 * u2, &s, &co);
+            gs[k] = r * co;
+            gs[k + 1] = r * s;
+        }
+        set_zero(m);
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            m(i, 0) = mkc(gs[2 * i], gs[2 * i + 1]);
+            m(i, 1) = mkc(gs[6 + 2 * i], gs[6 + 2 * i + 1]);
+        }
+        project_su3(m);
+    }
+    U.store(mu, par, h, convert<R>(m));
+}
+
+// U'(x) = U(x - s) (the global translation of Shift.cpp:109-160 on one periodic lattice).
+template <typename R, int NE>
+__global__ void k_shift(Geom g, LinkField<R, NE> src, LinkField<R, NE> dst, int s0, int s1, int s2, int s3) {
+    const int lt = blockIdx.y;
+    const int mu = lt >> 1, par = lt & 1;
+    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= g.Vh) return;
+    int c[4];
+    site_coords(g, par, (uint32_t)h, c);
+    const int s[4] = {s0, s1, s2, s3};
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        int v = c[d] - s[d];
+        if (v < 0) v += g.L[d];
+        c[d] = v;
+    }
+    const int spar = (c[0] + c[1] + c[2] + c[3]) & 1;
+    const int64_t slex = lex_of(g, c);
+    // raw element copy (no rebuild / re-encode for NE == 6)
+#pragma unroll
+    for (int e = 0; e < NE; e++) dst.p[dst.plane(mu, par, e) + h] = __ldg(src.p + src.plane(mu, spar, e) + (slex >> 1));
+}
+
+// projection_su3 of every link, in double (GaugeField.cpp:61-71).
+template <typename R, int NE>
+__global__ void k_reunitarize(Geom g, LinkField<R, NE> U) {
+    const int lt = blockIdx.y;
+    const int mu = lt >> 1, par = lt & 1;
+    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= g.Vh) return;
+    M3<double> u = convert<double>(U.load(mu, par, h));
+    project_su3(u);
+    U.store(mu, par, h, convert<R>(u));
+}
+
+// Staple field of one direction, written in AoS order (diagnostic entry point).
+template <typename R, int NE, int MU>
+__global__ void k_staple_field(Geom g, LinkField<R, NE> U, double2* out) {
+    const int par = blockIdx.y;
+    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= g.Vh) return;
+    int c[4];
+    site_coords(g, par, (uint32_t)h, c);
+    const int64_t lex = lex_of(g, c);
+    M3<R> A = staple<R, NE, MU, true>(g, U, c, lex, par);
+#pragma unroll
+    for (int e = 0; e < 9; e++) {
+        double2 v;
+        v.x = (double)A.e[e].re;
+        v.y = (double)A.e[e].im;
+        out[lex * 9 + e] = v;
+    }
+}
+
+}  // namespace qcb

@@ -1,0 +1,163 @@
+/*
+ * qcb.h -- C ABI of the B200 gauge-field hot path (libqcb.so).
+ *
+ * Plain pointers, sizes and opaque handles; no CUDA or C++ types cross it.  Every
+ * function returns 0 (QCB_OK) or a negative status, never throws, and records a
+ * message readable with qcb_last_error() (per host thread).  Work is ordered on the
+ * handle's CUDA stream; calls that return results to host memory synchronise it.
+ *
+ * Host link buffers use the "AoS" order of the reference's GaugeField interior and of
+ * the ILDG payload (src/gauge/GaugeField.h:27,49-56; src/io/ildg.cpp:87-106): sites
+ * lexicographic with x fastest and t slowest, then mu = x,y,z,t, then the row-major
+ * 3x3 complex matrix as (re, im) doubles -- V*4*9*2 doubles.
+ *
+ * Replaced reference interfaces are cited as path:line inside the reference tree.
+ */
+#ifndef QCB_H
+#define QCB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define QCB_OK 0
+#define QCB_EINVAL -1   /* invalid argument (sizes, parity, handle) */
+#define QCB_ENOMEM -2   /* device allocation failed or over the configured budget */
+#define QCB_EIO -3      /* file could not be opened / read / written */
+#define QCB_EFORMAT -4  /* LIME/ILDG structure or size mismatch */
+#define QCB_ECUDA -5    /* CUDA runtime error */
+#define QCB_ETIMEOUT -6 /* a bounded device or host wait ran out */
+#define QCB_ERANGE -7   /* a device-side cap was hit (e.g. heatbath attempt cap) */
+
+/* ---- storage formats ---- */
+#define QCB_PREC_F64 64
+#define QCB_PREC_F32 32
+#define QCB_STORE_18 0 /* full 3x3 complex matrix (18 reals) */
+#define QCB_STORE_12 1 /* first two rows (12 reals), third rebuilt in registers */
+
+typedef struct qcb_field_s* qcb_field;
+typedef struct qcb_flow_s* qcb_flow;
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char* qcb_last_error(void);
+/* Library build string (arch, version). */
+const char* qcb_version(void);
+/* Number of kernels this library has launched in this process. */
+uint64_t qcb_launch_count(void);
+
+/* ------------------------------------------------------------------ fields */
+/* Replaces GaugeField(const GeometryCB&) (src/gauge/GaugeField.h:30-43) and
+ * GeometryCB(int L) (src/geometry/GeometryCB.cpp:5-9): one periodic L[0]xL[1]xL[2]xL[3]
+ * lattice resident on the current CUDA device, every link set to the identity.  All
+ * extents must be even and >= 2.  prec: QCB_PREC_F64 / QCB_PREC_F32; store: QCB_STORE_*. */
+int qcb_field_create(const int L[4], int prec, int store, qcb_field* out);
+int qcb_field_destroy(qcb_field f);
+int qcb_field_info(qcb_field f, int L[4], int* prec, int* store, size_t* device_bytes);
+/* The CUDA stream (cudaStream_t) the handle's work is ordered on, and a way to set it. */
+void* qcb_field_stream(qcb_field f);
+int qcb_field_set_stream(qcb_field f, void* cuda_stream);
+int qcb_field_sync(qcb_field f);
+
+/* Host <-> device in AoS order (see top).  Replaces direct access to GaugeField::links
+ * (src/gauge/GaugeField.h:27).  `links` may be pageable or pinned host memory. */
+int qcb_field_upload_aos(qcb_field f, const double* links);
+int qcb_field_download_aos(qcb_field f, double* links);
+/* Same, from / to device memory (AoS doubles already on the field's device). */
+int qcb_field_upload_aos_device(qcb_field f, const double* d_links);
+int qcb_field_download_aos_device(qcb_field f, double* d_links);
+/* dst <- src (any precision / storage combination; same lattice). */
+int qcb_field_copy(qcb_field dst, qcb_field src);
+
+/* cold_start (src/gauge/GaugeField.cpp:23-33). */
+int qcb_cold_start(qcb_field f);
+/* hot_start (src/gauge/GaugeField.cpp:10-20): Haar-random SU(3) per link from a Philox
+ * stream keyed on seed (the reference's Householder-QR generator needs Eigen). */
+int qcb_hot_start(qcb_field f, uint64_t seed);
+/* project_field_su3 (src/gauge/GaugeField.cpp:61-71), column Gram-Schmidt in FP64. */
+int qcb_reunitarize(qcb_field f);
+/* max and mean over links of ||U U^dag - 1||_F (src/bin/test.cpp:47-93). */
+int qcb_unitarity(qcb_field f, double* max_err, double* mean_err);
+
+/* ------------------------------------------------------------------ global shift */
+/* shift_field (src/mpi/Shift.cpp:109-160) on one periodic lattice: U'(x) = U(x - s). */
+int qcb_shift(qcb_field f, const int s[4]);
+/* random_shift (src/mpi/Shift.cpp:163-186): draws s_d uniform in [0, n-1] with
+ * n = max_shift (or L[d] when max_shift <= 0) from a Philox stream keyed on (seed, idx),
+ * applies it and returns it in s_out (may be NULL). */
+int qcb_random_shift(qcb_field f, uint64_t seed, uint64_t idx, int max_shift, int s_out[4]);
+
+/* ------------------------------------------------------------------ heatbath */
+/* mpi::heatbathcb::sweep restricted to one (parity, mu) set (src/heatbath/heatbath_mpi.cpp:36-57,
+ * hit :10-33, heatbath.cpp:8-44).  Every link (x, mu) with parity(x) == parity receives
+ * n_hits Cabibbo-Marinari hits over the subgroups (0,1),(1,2),(0,2), with uniforms from a
+ * Philox stream keyed on seed and countered on (draw, link, sweep). */
+int qcb_hb_subsweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_t sweep, int parity, int mu);
+/* Full sweep: (parity 0, mu 0..3) then (parity 1, mu 0..3).  Replaces the pair
+ * sweep(EV); sweep(OD) of mpi::heatbathcb::samples (heatbath_mpi.cpp:60-75).  FP32 fields
+ * are reprojected to SU(3) in FP64 after each sweep. */
+int qcb_hb_sweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_t sweep);
+
+/* ------------------------------------------------------------------ observables */
+/* mean_plaquette_global (src/observables/observables_mpi.cpp:39-48). */
+int qcb_plaquette(qcb_field f, double* plaq);
+/* topo_q_e_clover_global (src/observables/observables_mpi.cpp:136-156): Q and E = sum(e)/V. */
+int qcb_clover_qe(qcb_field f, double* Q, double* E);
+
+/* ------------------------------------------------------------------ Wilson flow */
+/* GradientFlow(double eps, const GaugeField&, const GeometryCB&) (src/flow/gradient_flow.h:11-27,
+ * gradient_flow.cpp:12-13): a flow state owning its flowed field and RK3 buffers, of the
+ * given precision / storage (independent of src's), initialised as a copy of src. */
+int qcb_flow_create(qcb_field src, double eps, int prec, int store, qcb_flow* out);
+int qcb_flow_destroy(qcb_flow fl);
+/* GradientFlow::copy (gradient_flow.cpp:138). */
+int qcb_flow_copy(qcb_flow fl, qcb_field src);
+/* n x GradientFlow::rk3_step (gradient_flow.cpp:124-135); fused stages, ping-pong buffers. */
+int qcb_flow_rk3(qcb_flow fl, int n);
+/* topo_charge_flowed (src/observables/observables_mpi.cpp:159-186): copy src, then n_steps
+ * times { measure (Q, E) ; if not last: n_rk RK3 steps }; tQE receives 3*n_steps doubles
+ * (t, Q, E).  If plaq is non-NULL it receives n_steps plaquettes measured beside Q, E. */
+int qcb_flow_measure(qcb_flow fl, qcb_field src, int n_steps, int n_rk, double* tQE, double* plaq);
+/* The flowed field (GradientFlow::field_c); owned by the flow state. */
+qcb_field qcb_flow_field(qcb_flow fl);
+
+/* ------------------------------------------------------------------ ILDG */
+/* save_ildg_clime (src/io/ildg.cpp:34-136): LIME records "ildg-format" (MB=1, ME=1) and
+ * "ildg-binary-data" (MB=0, ME=1), big-endian FP64, site order t,z,y,x, mu = x,y,z,t. */
+int qcb_ildg_write(qcb_field f, const char* path);
+/* read_ildg_clime (src/io/ildg.cpp:138-237): finds "ildg-binary-data", checks its size
+ * against the lattice, reads 64- or 32-bit payloads (precision from the "ildg-format"
+ * record when present). */
+int qcb_ildg_read(qcb_field f, const char* path);
+/* Reads the lattice extents and precision of an ILDG file ("ildg-format" record). */
+int qcb_ildg_probe(const char* path, int L[4], int* precision);
+
+/* ------------------------------------------------------------------ instrumentation */
+/* Kernel classes timed by CUDA events recorded on the handle's stream around each launch. */
+#define QCB_K_HB 0
+#define QCB_K_FLOW 1
+#define QCB_K_PLAQ 2
+#define QCB_K_CLOVER 3
+#define QCB_K_OTHER 4
+#define QCB_K_NCLASS 5
+int qcb_timing_enable(qcb_field f, int on);
+/* Synchronises and returns (launches, total ms) for one kernel class since the last reset. */
+int qcb_timing_read(qcb_field f, int kclass, long* launches, double* total_ms);
+int qcb_timing_reset(qcb_field f);
+
+/* ------------------------------------------------------------------ diagnostics */
+/* Staple A(x, mu) of every site (src/gauge/GaugeField.cpp:74-97) into host AoS (V*9 complex). */
+int qcb_diag_staple(qcb_field f, int mu, double* out);
+/* exp_su3_luscher (src/su3/utils.cpp:145-193) of n matrices (n*9 complex) on the device. */
+int qcb_diag_exp_su3(const double* Z, int n, double coeff, int prec, double* out);
+/* n Philox4x32-10 blocks on the device: ctr word 0 = ctr[0] + i. */
+int qcb_diag_philox(const uint32_t ctr[4], const uint32_t key[2], int n, uint32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

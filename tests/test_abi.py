@@ -1,0 +1,79 @@
+"""The C ABI library loads and exports every symbol include/qcb.h declares (no GPU needed).
+Also exercises the host-only LIME/ILDG record parser (qcb_ildg_probe) on crafted files."""
+import os
+import re
+import struct
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "qcb.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(qcb_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(qcb):
+    lib = qcb.load_library()
+    names = declared_symbols()
+    assert len(names) >= 35
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_header(qcb):
+    assert sorted(qcb.exported_symbols()) == declared_symbols()
+
+
+def test_version_and_launch_counter(qcb):
+    assert b"sm_100a" in qcb.lib().qcb_version()
+    assert qcb.launch_count() >= 0
+
+
+def lime_record(rtype: bytes, payload: bytes, mb: bool, me: bool) -> bytes:
+    hdr = struct.pack(">IHBB Q", 0x456789AB, 1, (0x80 if mb else 0) | (0x40 if me else 0), 0, len(payload))
+    hdr = hdr.replace(b" ", b"")
+    hdr += rtype.ljust(128, b"\0")
+    assert len(hdr) == 144
+    pad = (-len(payload)) % 8
+    return hdr + payload + b"\0" * pad
+
+
+def ildg_xml(L, prec=64):
+    return ("<?xml version=\"1.0\" encoding=\"UTF-8\"?>\n<ildgFormat><version>1.0</version><field>su3gauge</field>"
+            f"<precision>{prec}</precision><lx>{L[0]}</lx><ly>{L[1]}</ly><lz>{L[2]}</lz><lt>{L[3]}</lt>"
+            "</ildgFormat>").encode()
+
+
+def test_ildg_probe_reads_format_record(qcb, tmp_path):
+    p = tmp_path / "a.ildg"
+    L = (4, 6, 2, 8)
+    V = L[0] * L[1] * L[2] * L[3]
+    p.write_bytes(lime_record(b"ildg-format", ildg_xml(L, 32), True, True) +
+                  lime_record(b"ildg-binary-data", b"\0" * (V * 72 * 4), False, True))
+    assert qcb.ildg_probe(str(p)) == (L, 32)
+
+
+def test_ildg_probe_errors(qcb, tmp_path):
+    with pytest.raises(qcb.QcbError) as e:
+        qcb.ildg_probe(str(tmp_path / "missing"))
+    assert e.value.code == -3
+    bad = tmp_path / "bad"
+    bad.write_bytes(b"\x12\x34" * 100)
+    with pytest.raises(qcb.QcbError) as e:
+        qcb.ildg_probe(str(bad))
+    assert e.value.code == -4
+    trunc = tmp_path / "trunc"
+    trunc.write_bytes(lime_record(b"ildg-format", ildg_xml((4, 4, 4, 4)), True, True)[:100])
+    with pytest.raises(qcb.QcbError) as e:
+        qcb.ildg_probe(str(trunc))
+    assert e.value.code == -4
+    noxml = tmp_path / "noxml"
+    noxml.write_bytes(lime_record(b"ildg-binary-data", b"\0" * 64, True, True))
+    with pytest.raises(qcb.QcbError) as e:
+        qcb.ildg_probe(str(noxml))
+    assert e.value.code == -4
