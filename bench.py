@@ -85,7 +85,13 @@ class Clocks:
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
-        self.idx = gpu_index
+        self.idx = str(gpu_index)
+        try:
+            import torch
+
+            self.idx = "GPU-" + str(torch.cuda.get_device_properties(gpu_index).uuid)
+        except Exception:
+            pass
         self.proc = None
         self.f = None
 
@@ -268,6 +274,14 @@ def run_ours(args, rank: int, world: int, local: int):
     f.hot_start(SEED_HOT)
     stream, e0, e1 = cuda_timer(qcb, f)
 
+    if args.only == "flow":
+        for i in range(args.warmup):
+            f.hb_sweep(BETA, N_HITS, SEED_HB, i)
+        for prec, store in ((64, 0), (32, 0), (32, 1)):
+            flow_block(qcb, f, prec, store, args.steps, 2, hbm_peak)
+        f.close()
+        return
+
     # ---------------- device-resident heatbath: warm-up, then K timed sweeps
     for i in range(args.warmup):
         f.hb_sweep(BETA, N_HITS, SEED_HB, i)
@@ -295,6 +309,10 @@ def run_ours(args, rank: int, world: int, local: int):
     achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
     traffic = profile_traffic("hb_subsweep_fp64_32x4")
     plaq = f.plaquette()
+
+    if args.only == "hb":
+        f.close()
+        return
 
     # ---------------- end to end through the C ABI with host buffers
     U_host = torch.empty(V * 72, dtype=torch.float64, pin_memory=True)
@@ -331,7 +349,7 @@ def run_ours(args, rank: int, world: int, local: int):
         flow[k]["speedup_vs_fp64"] = flow[k]["site_steps_per_s"] / flow["fp64"]["site_steps_per_s"]
 
     cpu = None
-    if rank == 0:
+    if rank == 0 and args.cpu_seconds > 0:
         orc = load_oracle()
         cpu = cpu_sample(orc, seconds=args.cpu_seconds)
 
@@ -367,7 +385,10 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="length of the CPU-baseline sample (0 skips it)")
+    ap.add_argument("--only", default="all", choices=["all", "hb", "flow"],
+                    help="run one part (used for ncu captures of a single kernel family)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -233,7 +233,7 @@ int download_to_staging(qcb_field_s* f, int bswap) {
 int flow_stage(qcb_flow_s* fl, int stage) {
     qcb_field_s* f = fl->fld;
     RET(ensure_alt(f));
-    const unsigned nb = 8u * blocks_for(f->g.Vh, 128);
+    const unsigned nb = 8u * blocks_for(f->g.Vh, QCB_FLOW_THREADS);
     const int rep = (f->prec == QCB_PREC_F32) ? 1 : 0;
     int r = QCB_OK;
     DISPATCH_FMT(
@@ -242,11 +242,11 @@ int flow_stage(qcb_flow_s* fl, int stage) {
             auto wout = view<R, NE>(f->alt, f->g.Vh);
             auto z = alg_view<R>(fl->z, f->g.Vh);
             if (stage == 1)
-                k_flow_stage<R, NE, 1><<<nb, 128, 0, f->stream>>>(f->g, win, wout, z, fl->eps, rep);
+                k_flow_stage<R, NE, 1><<<nb, QCB_FLOW_THREADS, 0, f->stream>>>(f->g, win, wout, z, fl->eps, rep);
             else if (stage == 2)
-                k_flow_stage<R, NE, 2><<<nb, 128, 0, f->stream>>>(f->g, win, wout, z, fl->eps, rep);
+                k_flow_stage<R, NE, 2><<<nb, QCB_FLOW_THREADS, 0, f->stream>>>(f->g, win, wout, z, fl->eps, rep);
             else
-                k_flow_stage<R, NE, 3><<<nb, 128, 0, f->stream>>>(f->g, win, wout, z, fl->eps, rep);
+                k_flow_stage<R, NE, 3><<<nb, QCB_FLOW_THREADS, 0, f->stream>>>(f->g, win, wout, z, fl->eps, rep);
         }));
     RET(r);
     void* t = f->links;
@@ -570,11 +570,11 @@ int qcb_hb_subsweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_
     if (!f) return fail(QCB_EINVAL, "null field");
     if (parity < 0 || parity > 1 || mu < 0 || mu > 3 || n_hits < 0 || !(beta > 0.0))
         return fail(QCB_EINVAL, "heatbath: parity in {0,1}, mu in 0..3, n_hits >= 0, beta > 0");
-    const unsigned nb = blocks_for(f->g.Vh, 128);
+    const unsigned nb = blocks_for(f->g.Vh, QCB_HB_THREADS);
     const int rep = (f->prec == QCB_PREC_F32) ? 1 : 0;
     int r = QCB_OK;
     DISPATCH_FMT(f->fmt, DISPATCH_MU(mu, r = launch(f, QCB_K_HB, [&] {
-                                          k_hb_subsweep<R, NE, MU><<<nb, 128, 0, f->stream>>>(
+                                          k_hb_subsweep<R, NE, MU><<<nb, QCB_HB_THREADS, 0, f->stream>>>(
                                               f->g, view<R, NE>(f->links, f->g.Vh), parity, beta, n_hits, seed,
                                               sweep, rep, f->d_err);
                                       })));
@@ -611,7 +611,8 @@ int qcb_flow_create(qcb_field src, double eps, int prec, int store, qcb_flow* ou
     qcb_flow_s* fl = new (std::nothrow) qcb_flow_s();
     if (!fl) return fail(QCB_ENOMEM, "host allocation");
     fl->eps = eps;
-    int r = field_new(src->L, prec, store, src->stream, &fl->fld);
+    // The flow owns its stream: it must outlive no other handle's resources.
+    int r = field_new(src->L, prec, store, nullptr, &fl->fld);
     if (r != QCB_OK) {
         delete fl;
         return r;

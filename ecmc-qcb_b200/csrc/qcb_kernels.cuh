@@ -57,14 +57,68 @@ __device__ __forceinline__ M3<R> staple(const Geom& g, const LinkField<R, NE>& U
     return A;
 }
 
+// Same staple with a runtime direction and a rolled nu loop: one code path for all four
+// directions (a single kernel then serves every link class without four unrolled copies
+// competing for the instruction cache).  The nu order is the reference's (ascending, skip mu).
+template <typename R, int NE>
+__device__ __forceinline__ M3<R> staple_rt(const Geom& g, const LinkField<R, NE>& U, const int c[4], int64_t lex,
+                                           int par, int mu) {
+    M3<R> A;
+    set_zero(A);
+    const int opp = par ^ 1;
+    const int64_t xmu = step_up(g, lex, c[mu], mu);
+#pragma unroll 1
+    for (int k = 0; k < 3; k++) {
+        const int nu = k < mu ? k : k + 1;
+        const int64_t xnu = step_up(g, lex, c[nu], nu);
+        const int64_t xmnu = step_dn(g, lex, c[nu], nu);
+        const int64_t xmumnu = step_dn(g, xmu, c[nu], nu);
+        {
+            M3<R> a = U.load_ro(nu, opp, xmu >> 1);
+            M3<R> b = U.load_ro(mu, opp, xnu >> 1);
+            M3<R> t = mul_na(a, b);
+            M3<R> d = U.load_ro(nu, par, lex >> 1);
+            acc_na(A, t, d);
+        }
+        {
+            M3<R> v1 = U.load_ro(mu, opp, xmnu >> 1);
+            M3<R> v0 = U.load_ro(nu, par, xmumnu >> 1);
+            M3<R> t = mul_nn(v1, v0);
+            M3<R> v2 = U.load_ro(nu, opp, xmnu >> 1);
+            acc_an(A, t, v2);
+        }
+    }
+    return A;
+}
+
+// Launch shapes (measured on B200, 32^4): 128-thread blocks; minimum resident blocks per SM
+// 3 for FP64 (<= 168 registers, no spills) and 4 for FP32 (<= 128 registers, no spills).
+#ifndef QCB_HB_THREADS
+#define QCB_HB_THREADS 128
+#endif
+#ifndef QCB_HB_MINB
+#define QCB_HB_MINB(R) (sizeof(R) == 8 ? 3 : 4)
+#endif
+#ifndef QCB_FLOW_THREADS
+#define QCB_FLOW_THREADS 128
+#endif
+#ifndef QCB_FLOW_MINB
+#define QCB_FLOW_MINB(R) (sizeof(R) == 8 ? 3 : 4)
+#endif
+#ifndef QCB_FLOW_RTMU
+#define QCB_FLOW_RTMU 1
+#endif
+
 // ------------------------------------------------------------------ heatbath
 struct Quat {
     double a0, a1, a2, a3;
 };
 
 // generate_su2_kp (src/heatbath/heatbath.cpp:8-36) + su2_step (:39-44).
-// The Kennedy-Pendleton loop has an attempt cap (never reached for beta*k > 1e-3); on the
-// cap the link keeps r = identity and the kernel raises DERR_KP_CAP.
+// The Kennedy-Pendleton loop is capped at KP_MAX_ATTEMPTS attempts, and a non-finite or
+// zero alpha = 2 beta k / 3 is rejected up front; in either case the subgroup element is the
+// identity (the link is left unchanged by this subgroup) and the kernel raises DERR_KP_CAP.
+constexpr int KP_MAX_ATTEMPTS = 4096;
 __device__ __forceinline__ Quat su2_step(double beta, Quat w, LinkStream& rng, int* err) {
     double k = sqrt(w.a0 * w.a0 + w.a1 * w.a1 + w.a2 * w.a2 + w.a3 * w.a3);
     double ik = 1.0 / k;
@@ -73,7 +127,8 @@ __device__ __forceinline__ Quat su2_step(double beta, Quat w, LinkStream& rng, i
     double m05a = -0.5 / alpha;
     double a0 = 1.0;
     bool ok = false;
-    for (int it = 0; it < (1 << 20); it++) {
+    const int cap = (alpha > 0.0 && isfinite(m05a)) ? KP_MAX_ATTEMPTS : 0;
+    for (int it = 0; it < cap; it++) {
         double delta = rng.next();
         double r1 = rng.next();
         double r2 = rng.next();
@@ -142,7 +197,7 @@ __device__ __forceinline__ void cm_subgroup(M3<R>& u, const M3<R>& A, double bet
 // (parity, mu); the staple is computed once per link, since it does not contain U(x,MU)
 // and is therefore identical for every hit (the reference recomputes it per hit).
 template <typename R, int NE, int MU>
-__global__ void __launch_bounds__(128) k_hb_subsweep(Geom g, LinkField<R, NE> U, int par, double beta, int n_hits,
+__global__ void __launch_bounds__(QCB_HB_THREADS, QCB_HB_MINB(R)) k_hb_subsweep(Geom g, LinkField<R, NE> U, int par, double beta, int n_hits,
                                                       uint64_t seed, uint32_t sweep, int reproject, int* err) {
     const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= g.Vh) return;
@@ -173,14 +228,25 @@ __global__ void __launch_bounds__(128) k_hb_subsweep(Geom g, LinkField<R, NE> U,
 //   stage 3: W' = exp(3/4 eps F - eps Z) W                          compute_w3
 // The whole field of forces is never materialised: Win is read-only for the launch and W'
 // goes to a second buffer (ping-pong), which is what makes force and update one pass.
-template <typename R, int NE, int STAGE, int MU>
+template <typename R, int NE, int STAGE>
 __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>& Win, const LinkField<R, NE>& Wout,
-                                          const AlgField<R>& Z, double eps, int par, int64_t h, int reproject) {
+                                          const AlgField<R>& Z, double eps, int mu, int par, int64_t h,
+                                          int reproject) {
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
     const int64_t lex = lex_of(g, c);
-    M3<R> A = staple<R, NE, MU, true>(g, Win, c, lex, par);
-    M3<R> u = Win.load_ro(MU, par, h);
+    M3<R> A;
+#if QCB_FLOW_RTMU
+    A = staple_rt<R, NE>(g, Win, c, lex, par, mu);
+#else
+    switch (mu) {
+        case 0: A = staple<R, NE, 0, true>(g, Win, c, lex, par); break;
+        case 1: A = staple<R, NE, 1, true>(g, Win, c, lex, par); break;
+        case 2: A = staple<R, NE, 2, true>(g, Win, c, lex, par); break;
+        default: A = staple<R, NE, 3, true>(g, Win, c, lex, par); break;
+    }
+#endif
+    M3<R> u = Win.load_ro(mu, par, h);
     M3<R> F = proj_lie(mul_nn(u, A));
 #pragma unroll
     for (int k = 0; k < 9; k++) F.e[k] = mkc<R>(-F.e[k].re, -F.e[k].im);  // proj_lie(-UA) = -proj_lie(UA)
@@ -189,9 +255,9 @@ __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>&
         const R c1 = (R)(0.25 * eps);
 #pragma unroll
         for (int k = 0; k < 9; k++) X.e[k] = scl(c1, F.e[k]);
-        Z.store(MU, par, h, F);
+        Z.store(mu, par, h, F);
     } else if (STAGE == 2) {
-        M3<R> z0 = Z.load(MU, par, h);
+        M3<R> z0 = Z.load(mu, par, h);
         const R a = (R)((8.0 / 9.0) * eps), b = (R)((17.0 / 36.0) * eps);
         const R a1 = (R)(8.0 / 9.0), b1 = (R)(17.0 / 36.0);
         M3<R> zn;
@@ -200,9 +266,9 @@ __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>&
             X.e[k] = scl(a, F.e[k]) - scl(b, z0.e[k]);
             zn.e[k] = scl(a1, F.e[k]) - scl(b1, z0.e[k]);
         }
-        Z.store(MU, par, h, zn);
+        Z.store(mu, par, h, zn);
     } else {
-        M3<R> z0 = Z.load(MU, par, h);
+        M3<R> z0 = Z.load(mu, par, h);
         const R a = (R)(0.75 * eps), b = (R)eps;
 #pragma unroll
         for (int k = 0; k < 9; k++) X.e[k] = scl(a, F.e[k]) - scl(b, z0.e[k]);
@@ -214,24 +280,19 @@ __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>&
         project_su3(wd);
         w = convert<R>(wd);
     }
-    Wout.store(MU, par, h, w);
+    Wout.store(mu, par, h, w);
 }
 
 // Grid: blockIdx.x = (site block) * 8 + (mu*2 + parity), so the 8 link classes of a block of
 // sites run together and share their neighbour links in L2.
 template <typename R, int NE, int STAGE>
-__global__ void __launch_bounds__(128) k_flow_stage(Geom g, LinkField<R, NE> Win, LinkField<R, NE> Wout,
-                                                     AlgField<R> Z, double eps, int reproject) {
+__global__ void __launch_bounds__(QCB_FLOW_THREADS, QCB_FLOW_MINB(R))
+    k_flow_stage(Geom g, LinkField<R, NE> Win, LinkField<R, NE> Wout, AlgField<R> Z, double eps, int reproject) {
     const int lt = blockIdx.x & 7;
     const int mu = lt >> 1, par = lt & 1;
     const int64_t h = (int64_t)(blockIdx.x >> 3) * blockDim.x + threadIdx.x;
     if (h >= g.Vh) return;
-    switch (mu) {
-        case 0: flow_link<R, NE, STAGE, 0>(g, Win, Wout, Z, eps, par, h, reproject); break;
-        case 1: flow_link<R, NE, STAGE, 1>(g, Win, Wout, Z, eps, par, h, reproject); break;
-        case 2: flow_link<R, NE, STAGE, 2>(g, Win, Wout, Z, eps, par, h, reproject); break;
-        default: flow_link<R, NE, STAGE, 3>(g, Win, Wout, Z, eps, par, h, reproject); break;
-    }
+    flow_link<R, NE, STAGE>(g, Win, Wout, Z, eps, mu, par, h, reproject);
 }
 
 // ------------------------------------------------------------------ reductions
