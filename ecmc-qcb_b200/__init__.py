@@ -82,6 +82,7 @@ def exported_symbols():
         "qcb_diag_staple": (i, [_vp, i, _vp]),
         "qcb_diag_exp_su3": (i, [_vp, i, d, i, _vp]),
         "qcb_diag_philox": (i, [C.POINTER(u32), C.POINTER(u32), i, C.POINTER(u32)]),
+        "qcb_plaquette_noalloc": (i, [_i4, _vp, _vp, _vp]),
     }
 
 
@@ -292,6 +293,12 @@ class GradientFlow:
                                       pl.ctypes.data if pl is not None else None))
         tqe = out.reshape(n_steps, 3)
         return (tqe, pl) if plaquette else tqe
+
+
+def plaquette_noalloc(L, d_links: int, d_out: int, stream: int = 0) -> None:
+    """Mean plaquette of caller-owned device links (parity-split FP64 layout) into d_out[0],
+    enqueued on `stream`; the library allocates nothing (see qcb_plaquette_noalloc in qcb.h)."""
+    _check(lib().qcb_plaquette_noalloc(_i4(*[int(v) for v in L]), _vp(d_links), _vp(d_out), _vp(stream)))
 
 
 def exp_su3(Z: np.ndarray, coeff: float, prec: int = PREC_F64) -> np.ndarray:

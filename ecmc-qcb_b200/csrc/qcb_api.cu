@@ -24,6 +24,8 @@ thread_local std::string g_err;
 std::atomic<uint64_t> g_launches{0};
 }  // namespace
 
+void qcb::note_launches(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+
 int qcb::fail(int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;

@@ -20,6 +20,8 @@ inline size_t link_bytes(int fmt, int64_t Vh) { return (size_t)8 * fmt_ne(fmt) *
 inline size_t alg_bytes(int fmt, int64_t Vh) { return (size_t)8 * 4 * (size_t)Vh * fmt_cbytes(fmt); }
 
 int fail(int code, const char* fmt, ...);
+// Adds n to the process-wide kernel launch counter reported by qcb_launch_count().
+void note_launches(int n);
 
 struct TimedLaunch {
     int kclass;

@@ -156,6 +156,24 @@ int qcb_diag_exp_su3(const double* Z, int n, double coeff, int prec, double* out
 /* n Philox4x32-10 blocks on the device: ctr word 0 = ctr[0] + i. */
 int qcb_diag_philox(const uint32_t ctr[4], const uint32_t key[2], int n, uint32_t* out);
 
+/* ------------------------------------------------------------------ allocation-free entry */
+/* No counterpart in the reference (its plaquette, observables_mpi.cpp:39-48, runs on host
+ * memory).  For callers that cannot let a library allocate device memory -- code inside a
+ * framework that owns all device memory through its own pool, hosts that forbid allocation
+ * after start-up, loops that must not hit the allocator's implicit synchronisation -- this
+ * computes the mean plaquette of links the caller already holds in device memory and writes
+ * it to device memory the caller provides (d_plaq[0]), enqueued on `stream` (NULL = legacy
+ * default stream), without calling cudaMalloc, cudaFree or any allocating routine.
+ * d_links: FP64 links in the parity-split layout of a QCB_PREC_F64 / QCB_STORE_18 field:
+ *   complex element (row r, col c) of link (x, mu) at d_links[2*(((mu*2 + p)*9 + 3r + c)*V/2 + lex(x)/2)]
+ *   (+1 for the imaginary part), lex(x) = x0 + L0*(x1 + L1*(x2 + L2*x3)), p = (x0+x1+x2+x3) mod 2.
+ * Limits: even extents >= 2, volume <= 2^30 sites.  Scratch: a fixed static device array of
+ * 2*148*8 doubles (18.5 KiB) that every GPU loading the library holds until exit; all calls
+ * share it and it keeps the last call's contents, so calls that overlap on the GPU race.  The
+ * first call on a device looks the array's address up (cudaGetSymbolAddress) with that device
+ * current; make it before any stream capture on that device. */
+int qcb_plaquette_noalloc(const int L[4], const double* d_links, double* d_plaq, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
