@@ -83,6 +83,19 @@ def exported_symbols():
         "qcb_diag_exp_su3": (i, [_vp, i, d, i, _vp]),
         "qcb_diag_philox": (i, [C.POINTER(u32), C.POINTER(u32), i, C.POINTER(u32)]),
         "qcb_plaquette_noalloc": (i, [_i4, _vp, _vp, _vp]),
+        "qcb_batch_create": (i, [i, C.POINTER(C.c_int), pd, C.POINTER(u64), i, i, C.POINTER(_vp)]),
+        "qcb_batch_destroy": (i, [_vp]),
+        "qcb_batch_info": (i, [_vp, pi, pi, pi, pi, C.POINTER(u32)]),
+        "qcb_batch_stream": (_vp, [_vp]),
+        "qcb_batch_hot_start": (i, [_vp]),
+        "qcb_batch_cold_start": (i, [_vp]),
+        "qcb_batch_sweep": (i, [_vp, i, i]),
+        "qcb_batch_sync": (i, [_vp]),
+        "qcb_batch_plaquette": (i, [_vp, pd]),
+        "qcb_batch_upload_aos": (i, [_vp, i, _vp]),
+        "qcb_batch_download_aos": (i, [_vp, i, _vp]),
+        "qcb_batch_set_variant": (i, [_vp, i]),
+        "qcb_batch_tune": (i, [_vp, i, i, i, pi, pd]),
     }
 
 
@@ -247,6 +260,77 @@ class GaugeField:
 
     def timing_reset(self) -> None:
         _check(lib().qcb_timing_reset(self.h))
+
+
+class Batch:
+    """Many independent heatbath chains of uneven size and beta on one GPU (CUDA-graph sweeps)."""
+
+    def __init__(self, Ls, betas, seeds, prec: int = PREC_F64, store: int = STORE_18):
+        n = len(Ls)
+        assert len(betas) == n and len(seeds) == n
+        self.Ls = [tuple(int(v) for v in L) for L in Ls]
+        Lflat = (C.c_int * (4 * n))(*[v for L in self.Ls for v in L])
+        b = (C.c_double * n)(*[float(x) for x in betas])
+        sd = (C.c_uint64 * n)(*[int(x) for x in seeds])
+        h = _vp()
+        _check(lib().qcb_batch_create(n, Lflat, b, sd, int(prec), int(store), C.byref(h)))
+        self.h, self.n = h, n
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().qcb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return lib().qcb_batch_stream(self.h) or 0
+
+    def info(self):
+        n, p, st, v = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        sw = C.c_uint32()
+        _check(lib().qcb_batch_info(self.h, C.byref(n), C.byref(p), C.byref(st), C.byref(v), C.byref(sw)))
+        return {"n": n.value, "prec": p.value, "store": st.value, "variant": v.value, "sweep": sw.value}
+
+    def hot_start(self) -> None:
+        _check(lib().qcb_batch_hot_start(self.h))
+
+    def cold_start(self) -> None:
+        _check(lib().qcb_batch_cold_start(self.h))
+
+    def sweep(self, n_hits: int, n_sweeps: int = 1) -> None:
+        _check(lib().qcb_batch_sweep(self.h, int(n_hits), int(n_sweeps)))
+
+    def sync(self) -> None:
+        _check(lib().qcb_batch_sync(self.h))
+
+    def plaquette(self) -> np.ndarray:
+        out = np.empty(self.n)
+        _check(lib().qcb_batch_plaquette(self.h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def upload(self, i: int, U: np.ndarray) -> None:
+        U = np.ascontiguousarray(U, dtype=np.complex128)
+        _check(lib().qcb_batch_upload_aos(self.h, int(i), U.ctypes.data))
+
+    def download(self, i: int) -> np.ndarray:
+        out = np.empty((volume(self.Ls[i]), 4, 3, 3), dtype=np.complex128)
+        _check(lib().qcb_batch_download_aos(self.h, int(i), out.ctypes.data))
+        return out
+
+    def set_variant(self, v: int) -> None:
+        _check(lib().qcb_batch_set_variant(self.h, int(v)))
+
+    def tune(self, n_hits: int, n_trial: int = 2, allow_store_change: bool = False):
+        v = C.c_int()
+        ms = (C.c_double * 4)()
+        _check(lib().qcb_batch_tune(self.h, int(n_hits), int(n_trial), 1 if allow_store_change else 0, C.byref(v), ms))
+        return v.value, list(ms)
 
 
 def ildg_probe(path: str):

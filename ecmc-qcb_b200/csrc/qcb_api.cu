@@ -14,7 +14,7 @@
 #include <string>
 
 #include "qcb_internal.h"
-#include "qcb_kernels.cuh"
+#include "qcb_ops.h"
 
 using namespace qcb;
 
@@ -22,7 +22,18 @@ using namespace qcb;
 namespace {
 thread_local std::string g_err;
 std::atomic<uint64_t> g_launches{0};
+int g_sm_count = 0;
 }  // namespace
+
+int qcb::sm_count() {
+    if (g_sm_count == 0) {
+        int dev = 0, n = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+        g_sm_count = n;
+    }
+    return g_sm_count;
+}
 
 void qcb::note_launches(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 
@@ -41,72 +52,13 @@ int qcb::fail(int code, const char* fmt, ...) {
         cudaError_t e_ = (call);                                                                 \
         if (e_ != cudaSuccess) return fail(QCB_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
-#define RET(call)                \
-    do {                         \
-        int r_ = (call);         \
+#define RET(call)                    \
+    do {                             \
+        int r_ = (call);             \
         if (r_ != QCB_OK) return r_; \
     } while (0)
 
-// Format dispatch: instantiates BODY with R / NE for the field's storage format.
-#define DISPATCH_FMT(fmt, ...)                \
-    switch (fmt) {                            \
-        case FMT_D18: {                       \
-            typedef double R;                 \
-            constexpr int NE = 9;             \
-            __VA_ARGS__;                      \
-        } break;                              \
-        case FMT_D12: {                       \
-            typedef double R;                 \
-            constexpr int NE = 6;             \
-            __VA_ARGS__;                      \
-        } break;                              \
-        case FMT_F18: {                       \
-            typedef float R;                  \
-            constexpr int NE = 9;             \
-            __VA_ARGS__;                      \
-        } break;                              \
-        default: {                            \
-            typedef float R;                  \
-            constexpr int NE = 6;             \
-            __VA_ARGS__;                      \
-        } break;                              \
-    }
-#define DISPATCH_MU(mu, ...)       \
-    switch (mu) {                  \
-        case 0: {                  \
-            constexpr int MU = 0;  \
-            __VA_ARGS__;           \
-        } break;                   \
-        case 1: {                  \
-            constexpr int MU = 1;  \
-            __VA_ARGS__;           \
-        } break;                   \
-        case 2: {                  \
-            constexpr int MU = 2;  \
-            __VA_ARGS__;           \
-        } break;                   \
-        default: {                 \
-            constexpr int MU = 3;  \
-            __VA_ARGS__;           \
-        } break;                   \
-    }
-
 namespace {
-
-template <typename R, int NE>
-LinkField<R, NE> view(void* p, int64_t Vh) {
-    LinkField<R, NE> f;
-    f.p = (typename LinkField<R, NE>::C2*)p;
-    f.Vh = Vh;
-    return f;
-}
-template <typename R>
-AlgField<R> alg_view(void* p, int64_t Vh) {
-    AlgField<R> a;
-    a.p = (typename AlgField<R>::C2*)p;
-    a.Vh = Vh;
-    return a;
-}
 
 inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 // Grid size of the grid-stride reduction kernels: bounded so that the partial vectors
@@ -136,8 +88,8 @@ int launch(qcb_field_s* f, int kclass, Fn&& fn) {
         b = get_event(f);
         CK(cudaEventRecord(a, f->stream));
     }
-    fn();
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = fn();
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return fail(QCB_ECUDA, "kernel launch: %s", cudaGetErrorString(e));
     g_launches.fetch_add(1, std::memory_order_relaxed);
     if (f->timing) {
@@ -180,30 +132,23 @@ int check_err_flag(qcb_field_s* f) {
 
 // reduction of nb partial vectors of nv doubles into dst (device)
 int finalize(qcb_field_s* f, int nb, int nv, unsigned max_mask, double* dst) {
-    return launch(f, QCB_K_OTHER, [&] { k_finalize<<<1, 256, 0, f->stream>>>(f->partials, nb, nv, max_mask, dst); });
+    return launch(f, QCB_K_OTHER, [&] {
+        k_finalize<<<1, 256, 0, f->stream>>>(f->partials, nb, nv, max_mask, dst);
+        return cudaGetLastError();
+    });
 }
 
 // --- enqueue helpers (no host synchronisation) --------------------------------------
 int enq_plaquette(qcb_field_s* f, double* dst) {
     const unsigned nbx = red_blocks(f->g.Vh, 256);
     RET(ensure_partials(f, (size_t)nbx * 2));
-    int r = QCB_OK;
-    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_PLAQ, [&] {
-                     k_plaquette<R, NE><<<dim3(nbx, 2), 256, 0, f->stream>>>(f->g, view<R, NE>(f->links, f->g.Vh),
-                                                                                f->partials);
-                 }));
-    RET(r);
+    RET(launch(f, QCB_K_PLAQ, [&] { return fmt_ops(f->fmt).plaquette(f->g, f->links, f->partials, nbx, f->stream); }));
     return finalize(f, (int)(nbx * 2), 1, 0u, dst);
 }
 int enq_clover(qcb_field_s* f, double* dst) {
     const unsigned nbx = red_blocks(f->g.Vh, 128);
     RET(ensure_partials(f, (size_t)nbx * 6 * 2));
-    int r = QCB_OK;
-    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_CLOVER, [&] {
-                     k_clover_qe<R, NE><<<dim3(nbx, 6), 128, 0, f->stream>>>(f->g, view<R, NE>(f->links, f->g.Vh),
-                                                                                f->partials);
-                 }));
-    RET(r);
+    RET(launch(f, QCB_K_CLOVER, [&] { return fmt_ops(f->fmt).clover(f->g, f->links, f->partials, nbx, f->stream); }));
     return finalize(f, (int)(nbx * 6), 2, 0u, dst);
 }
 
@@ -214,43 +159,40 @@ int read_results(qcb_field_s* f, int n) {
 }
 
 int upload_from_staging(qcb_field_s* f, int bswap) {
-    int r = QCB_OK;
-    const unsigned nb = blocks_for(f->g.V * 4, 256);
-    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
-                     k_aos_to_soa<R, NE><<<nb, 256, 0, f->stream>>>(f->g, f->staging, view<R, NE>(f->links, f->g.Vh),
-                                                                    bswap);
-                 }));
-    return r;
+    return launch(f, QCB_K_OTHER,
+                  [&] { return fmt_ops(f->fmt).aos_to_soa(f->g, f->staging, f->links, bswap, f->stream); });
 }
 int download_to_staging(qcb_field_s* f, int bswap) {
-    int r = QCB_OK;
-    const unsigned nb = blocks_for(f->g.V * 4, 256);
-    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
-                     k_soa_to_aos<R, NE><<<nb, 256, 0, f->stream>>>(f->g, view<R, NE>(f->links, f->g.Vh), f->staging,
-                                                                    bswap);
-                 }));
-    return r;
+    return launch(f, QCB_K_OTHER,
+                  [&] { return fmt_ops(f->fmt).soa_to_aos(f->g, f->links, f->staging, bswap, f->stream); });
 }
 
-int flow_stage(qcb_flow_s* fl, int stage) {
+// Work list of a single field (descriptor passed by value).
+WorkList single_list(qcb_field_s* f) {
+    WorkList w;
+    w.one.g = f->g;
+    w.one.links = f->links;
+    w.one.links_out = f->alt;
+    w.one.nb_begin = 0;
+    w.one.nb = (int)((f->g.Vh + TILE - 1) / TILE);
+    w.one.flip = 0;
+    w.nb_total = w.one.nb;
+    w.nlat = 1;
+    return w;
+}
+
+// One RK3 step on the flow's field: stage 1 reads links and writes alt, stage 2 the reverse,
+// stage 3 links -> alt again; the buffers then swap so that links holds the result.
+int flow_step(qcb_flow_s* fl) {
     qcb_field_s* f = fl->fld;
     RET(ensure_alt(f));
-    const unsigned nb = 8u * blocks_for(f->g.Vh, QCB_FLOW_THREADS);
     const int rep = (f->prec == QCB_PREC_F32) ? 1 : 0;
-    int r = QCB_OK;
-    DISPATCH_FMT(
-        f->fmt, r = launch(f, QCB_K_FLOW, [&] {
-            auto win = view<R, NE>(f->links, f->g.Vh);
-            auto wout = view<R, NE>(f->alt, f->g.Vh);
-            auto z = alg_view<R>(fl->z, f->g.Vh);
-            if (stage == 1)
-                k_flow_stage<R, NE, 1><<<nb, QCB_FLOW_THREADS, 0, f->stream>>>(f->g, win, wout, z, fl->eps, rep);
-            else if (stage == 2)
-                k_flow_stage<R, NE, 2><<<nb, QCB_FLOW_THREADS, 0, f->stream>>>(f->g, win, wout, z, fl->eps, rep);
-            else
-                k_flow_stage<R, NE, 3><<<nb, QCB_FLOW_THREADS, 0, f->stream>>>(f->g, win, wout, z, fl->eps, rep);
-        }));
-    RET(r);
+    for (int stage = 1; stage <= 3; stage++) {
+        void* win = (stage == 2) ? f->alt : f->links;
+        void* wout = (stage == 2) ? f->links : f->alt;
+        RET(launch(f, QCB_K_FLOW,
+                   [&] { return fmt_ops(f->fmt).flow1(f->g, win, wout, fl->z, fl->eps, stage, rep, f->stream); }));
+    }
     void* t = f->links;
     f->links = f->alt;
     f->alt = t;
@@ -327,6 +269,31 @@ __global__ void qcb::k_finalize(const double* partials, int nb, int nv, unsigned
             __syncthreads();
         }
         if (threadIdx.x == 0) out[k] = sm[0];
+        __syncthreads();
+    }
+}
+
+// Per-lattice deterministic sums of tile partials (one block per lattice, fixed order).
+__global__ void qcb::k_lat_finalize(const LatDesc* __restrict__ lats, const LatDesc one,
+                                    const double* __restrict__ partials, int m, int nv, int scale_mode, double* out) {
+    __shared__ double sm[256];
+    const LatDesc* d = lats ? lats + blockIdx.x : &one;
+    const int t0 = m * d->nb_begin, nt = m * d->nb;
+    for (int k = 0; k < nv; k++) {
+        double acc = 0.0;
+        for (int i = threadIdx.x; i < nt; i += 256) acc += partials[(size_t)(t0 + i) * nv + k];
+        sm[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = 128; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            double v = sm[0];
+            if (scale_mode == 1) v /= 6.0 * (double)d->g.V;
+            if (scale_mode == 2 && k == 1) v /= (double)d->g.V;
+            out[(size_t)blockIdx.x * nv + k] = v;
+        }
         __syncthreads();
     }
 }
@@ -438,23 +405,13 @@ int qcb_field_download_aos(qcb_field f, double* links) {
 }
 int qcb_field_upload_aos_device(qcb_field f, const double* d_links) {
     if (!f || !d_links) return fail(QCB_EINVAL, "null argument");
-    int r = QCB_OK;
-    const unsigned nb = blocks_for(f->g.V * 4, 256);
-    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
-                     k_aos_to_soa<R, NE><<<nb, 256, 0, f->stream>>>(f->g, (const double2*)d_links,
-                                                                    view<R, NE>(f->links, f->g.Vh), 0);
-                 }));
-    return r;
+    return launch(f, QCB_K_OTHER,
+                  [&] { return fmt_ops(f->fmt).aos_to_soa(f->g, (const double2*)d_links, f->links, 0, f->stream); });
 }
 int qcb_field_download_aos_device(qcb_field f, double* d_links) {
     if (!f || !d_links) return fail(QCB_EINVAL, "null argument");
-    int r = QCB_OK;
-    const unsigned nb = blocks_for(f->g.V * 4, 256);
-    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
-                     k_soa_to_aos<R, NE><<<nb, 256, 0, f->stream>>>(f->g, view<R, NE>(f->links, f->g.Vh),
-                                                                    (double2*)d_links, 0);
-                 }));
-    return r;
+    return launch(f, QCB_K_OTHER,
+                  [&] { return fmt_ops(f->fmt).soa_to_aos(f->g, f->links, (double2*)d_links, 0, f->stream); });
 }
 
 int qcb_field_copy(qcb_field dst, qcb_field src) {
@@ -475,56 +432,32 @@ int qcb_field_copy(qcb_field dst, qcb_field src) {
         return QCB_OK;
     }
     RET(ensure_staging(dst));
-    int r = QCB_OK;
-    const unsigned nb = blocks_for(dst->g.V * 4, 256);
-    DISPATCH_FMT(src->fmt, r = launch(dst, QCB_K_OTHER, [&] {
-                     k_soa_to_aos<R, NE><<<nb, 256, 0, dst->stream>>>(src->g, view<R, NE>(src->links, src->g.Vh),
-                                                                      dst->staging, 0);
-                 }));
-    RET(r);
+    RET(launch(dst, QCB_K_OTHER,
+               [&] { return fmt_ops(src->fmt).soa_to_aos(src->g, src->links, dst->staging, 0, dst->stream); }));
     return upload_from_staging(dst, 0);
 }
 
 int qcb_cold_start(qcb_field f) {
     if (!f) return fail(QCB_EINVAL, "null field");
-    int r = QCB_OK;
-    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
-                     k_start<R, NE><<<dim3(blocks_for(f->g.Vh, 128), 8), 128, 0, f->stream>>>(
-                         f->g, view<R, NE>(f->links, f->g.Vh), 0, 0ull);
-                 }));
-    return r;
+    return launch(f, QCB_K_OTHER, [&] { return fmt_ops(f->fmt).start(f->g, f->links, 0, 0ull, f->stream); });
 }
 
 int qcb_hot_start(qcb_field f, uint64_t seed) {
     if (!f) return fail(QCB_EINVAL, "null field");
-    int r = QCB_OK;
-    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
-                     k_start<R, NE><<<dim3(blocks_for(f->g.Vh, 128), 8), 128, 0, f->stream>>>(
-                         f->g, view<R, NE>(f->links, f->g.Vh), 1, seed);
-                 }));
-    return r;
+    return launch(f, QCB_K_OTHER, [&] { return fmt_ops(f->fmt).start(f->g, f->links, 1, seed, f->stream); });
 }
 
 int qcb_reunitarize(qcb_field f) {
     if (!f) return fail(QCB_EINVAL, "null field");
-    int r = QCB_OK;
-    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
-                     k_reunitarize<R, NE><<<dim3(blocks_for(f->g.Vh, 128), 8), 128, 0, f->stream>>>(
-                         f->g, view<R, NE>(f->links, f->g.Vh));
-                 }));
-    return r;
+    return launch(f, QCB_K_OTHER, [&] { return fmt_ops(f->fmt).reunitarize(f->g, f->links, f->stream); });
 }
 
 int qcb_unitarity(qcb_field f, double* max_err, double* mean_err) {
     if (!f) return fail(QCB_EINVAL, "null field");
     const unsigned nbx = red_blocks(f->g.Vh, 256);
     RET(ensure_partials(f, (size_t)nbx * 8 * 2));
-    int r = QCB_OK;
-    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
-                     k_unitarity<R, NE><<<dim3(nbx, 8), 256, 0, f->stream>>>(f->g, view<R, NE>(f->links, f->g.Vh),
-                                                                                f->partials);
-                 }));
-    RET(r);
+    RET(launch(f, QCB_K_OTHER,
+               [&] { return fmt_ops(f->fmt).unitarity(f->g, f->links, f->partials, nbx, f->stream); }));
     RET(finalize(f, (int)(nbx * 8), 2, 1u, f->d_res));
     RET(read_results(f, 2));
     if (max_err) *max_err = f->h_res[0];
@@ -542,13 +475,7 @@ int qcb_shift(qcb_field f, const int s[4]) {
     }
     if (!any) return QCB_OK;
     RET(ensure_alt(f));
-    int r = QCB_OK;
-    DISPATCH_FMT(f->fmt, r = launch(f, QCB_K_OTHER, [&] {
-                     k_shift<R, NE><<<dim3(blocks_for(f->g.Vh, 128), 8), 128, 0, f->stream>>>(
-                         f->g, view<R, NE>(f->links, f->g.Vh), view<R, NE>(f->alt, f->g.Vh), sm[0], sm[1], sm[2],
-                         sm[3]);
-                 }));
-    RET(r);
+    RET(launch(f, QCB_K_OTHER, [&] { return fmt_ops(f->fmt).shift(f->g, f->links, f->alt, sm, f->stream); }));
     void* t = f->links;
     f->links = f->alt;
     f->alt = t;
@@ -572,15 +499,11 @@ int qcb_hb_subsweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_
     if (!f) return fail(QCB_EINVAL, "null field");
     if (parity < 0 || parity > 1 || mu < 0 || mu > 3 || n_hits < 0 || !(beta > 0.0))
         return fail(QCB_EINVAL, "heatbath: parity in {0,1}, mu in 0..3, n_hits >= 0, beta > 0");
-    const unsigned nb = blocks_for(f->g.Vh, QCB_HB_THREADS);
     const int rep = (f->prec == QCB_PREC_F32) ? 1 : 0;
-    int r = QCB_OK;
-    DISPATCH_FMT(f->fmt, DISPATCH_MU(mu, r = launch(f, QCB_K_HB, [&] {
-                                          k_hb_subsweep<R, NE, MU><<<nb, QCB_HB_THREADS, 0, f->stream>>>(
-                                              f->g, view<R, NE>(f->links, f->g.Vh), parity, beta, n_hits, seed,
-                                              sweep, rep, f->d_err);
-                                      })));
-    return r;
+    return launch(f, QCB_K_HB, [&] {
+        return fmt_ops(f->fmt).hb1(f->g, f->links, parity, mu, -0.75 / beta, n_hits, seed, sweep, rep, f->d_err,
+                                   f->stream);
+    });
 }
 
 int qcb_hb_sweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_t sweep) {
@@ -652,11 +575,7 @@ int qcb_flow_copy(qcb_flow fl, qcb_field src) {
 
 int qcb_flow_rk3(qcb_flow fl, int n) {
     if (!fl || n < 0) return fail(QCB_EINVAL, "invalid argument");
-    for (int i = 0; i < n; i++) {
-        RET(flow_stage(fl, 1));
-        RET(flow_stage(fl, 2));
-        RET(flow_stage(fl, 3));
-    }
+    for (int i = 0; i < n; i++) RET(flow_step(fl));
     return QCB_OK;
 }
 
@@ -734,13 +653,8 @@ int qcb_timing_reset(qcb_field f) {
 int qcb_diag_staple(qcb_field f, int mu, double* out) {
     if (!f || !out || mu < 0 || mu > 3) return fail(QCB_EINVAL, "invalid argument");
     RET(ensure_staging(f));
-    int r = QCB_OK;
-    DISPATCH_FMT(f->fmt, DISPATCH_MU(mu, r = launch(f, QCB_K_OTHER, [&] {
-                                          k_staple_field<R, NE, MU><<<dim3(blocks_for(f->g.Vh, 128), 2), 128, 0,
-                                                                      f->stream>>>(
-                                              f->g, view<R, NE>(f->links, f->g.Vh), f->staging);
-                                      })));
-    RET(r);
+    RET(launch(f, QCB_K_OTHER,
+               [&] { return fmt_ops(f->fmt).staple_field(f->g, f->links, mu, f->staging, f->stream); }));
     CK(cudaMemcpyAsync(out, f->staging, (size_t)f->g.V * 9 * sizeof(double2), cudaMemcpyDeviceToHost, f->stream));
     CK(cudaStreamSynchronize(f->stream));
     return QCB_OK;

@@ -114,20 +114,21 @@ struct Quat {
     double a0, a1, a2, a3;
 };
 
-// generate_su2_kp (src/heatbath/heatbath.cpp:8-36) + su2_step (:39-44).
-// The Kennedy-Pendleton loop is capped at KP_MAX_ATTEMPTS attempts, and a non-finite or
-// zero alpha = 2 beta k / 3 is rejected up front; in either case the subgroup element is the
-// identity (the link is left unchanged by this subgroup) and the kernel raises DERR_KP_CAP.
+// generate_su2_kp (src/heatbath/heatbath.cpp:8-36) + su2_step (:39-44), drawing in the
+// reference's order: (delta, r1, r2, r3) per Kennedy-Pendleton attempt, then (u_phi, u_cos).
+// With c_alpha = -0.75/beta, -0.5/alpha = c_alpha / k (alpha = 2 beta k / 3), so one rsqrt
+// gives both v = w/k and the attempt scale.
+// The loop is capped at KP_MAX_ATTEMPTS attempts and a non-finite or non-negative scale is
+// rejected up front; in either case the subgroup element is the identity (the link is left
+// unchanged by this subgroup) and the kernel raises DERR_KP_CAP.
 constexpr int KP_MAX_ATTEMPTS = 4096;
-__device__ __forceinline__ Quat su2_step(double beta, Quat w, LinkStream& rng, int* err) {
-    double k = sqrt(w.a0 * w.a0 + w.a1 * w.a1 + w.a2 * w.a2 + w.a3 * w.a3);
-    double ik = 1.0 / k;
-    Quat v = {w.a0 * ik, w.a1 * ik, w.a2 * ik, w.a3 * ik};
-    double alpha = beta * k * 2.0 / 3.0;
-    double m05a = -0.5 / alpha;
+__device__ __forceinline__ Quat su2_step(double c_alpha, Quat w, LinkStream& rng, int* err) {
+    const double ik = rsqrt(w.a0 * w.a0 + w.a1 * w.a1 + w.a2 * w.a2 + w.a3 * w.a3);  // 1/k
+    const Quat v = {w.a0 * ik, w.a1 * ik, w.a2 * ik, w.a3 * ik};
+    const double m05a = c_alpha * ik;  // -0.5 / alpha
     double a0 = 1.0;
     bool ok = false;
-    const int cap = (alpha > 0.0 && isfinite(m05a)) ? KP_MAX_ATTEMPTS : 0;
+    const int cap = (m05a < 0.0 && isfinite(m05a)) ? KP_MAX_ATTEMPTS : 0;
     for (int it = 0; it < cap; it++) {
         double delta = rng.next();
         double r1 = rng.next();
@@ -145,25 +146,24 @@ __device__ __forceinline__ Quat su2_step(double beta, Quat w, LinkStream& rng, i
         atomicOr(err, (int)DERR_KP_CAP);
         return Quat{1.0, 0.0, 0.0, 0.0};
     }
-    double rs = sqrt(1.0 - a0 * a0);
-    double uphi = rng.next();
-    double cos_t = 2.0 * rng.next() - 1.0;
-    double sin_t = sqrt(1.0 - cos_t * cos_t);
+    const double rs = sqrt(1.0 - a0 * a0);
+    const double uphi = rng.next();
+    const double cos_t = 2.0 * rng.next() - 1.0;
+    const double sin_t = sqrt(1.0 - cos_t * cos_t);
     double sp, cp;
     sincospi(2.0 * uphi, &sp, &cp);
-    Quat x = {a0, rs * sin_t * cp, rs * sin_t * sp, rs * cos_t};
+    const Quat x = {a0, rs * sin_t * cp, rs * sin_t * sp, rs * cos_t};
     // mult(x, adj(v))  (src/su3/utils.cpp:53-63)
-    Quat q = {x.a0 * v.a0 + x.a1 * v.a1 + x.a2 * v.a2 + x.a3 * v.a3,
-              -x.a0 * v.a1 + x.a1 * v.a0 - x.a2 * v.a3 + x.a3 * v.a2,
-              -x.a0 * v.a2 + x.a1 * v.a3 + x.a2 * v.a0 - x.a3 * v.a1,
-              -x.a0 * v.a3 - x.a1 * v.a2 + x.a2 * v.a1 + x.a3 * v.a0};
-    return q;
+    return Quat{x.a0 * v.a0 + x.a1 * v.a1 + x.a2 * v.a2 + x.a3 * v.a3,
+                -x.a0 * v.a1 + x.a1 * v.a0 - x.a2 * v.a3 + x.a3 * v.a2,
+                -x.a0 * v.a2 + x.a1 * v.a3 + x.a2 * v.a0 - x.a3 * v.a1,
+                -x.a0 * v.a3 - x.a1 * v.a2 + x.a2 * v.a1 + x.a3 * v.a0};
 }
 
 // One Cabibbo-Marinari subgroup update of u in place (src/heatbath/heatbath_mpi.cpp:14-32):
 // w = quaternion of the (I,J) block of W = u*A, r = su2_step(w), u <- embed_{IJ}(r) * u.
 template <typename R, int I, int J>
-__device__ __forceinline__ void cm_subgroup(M3<R>& u, const M3<R>& A, double beta, LinkStream& rng, int* err) {
+__device__ __forceinline__ void cm_subgroup(M3<R>& u, const M3<R>& A, double c_alpha, LinkStream& rng, int* err) {
     Cx<R> wii = mkc<R>(0, 0), wij = mkc<R>(0, 0), wji = mkc<R>(0, 0), wjj = mkc<R>(0, 0);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -175,7 +175,7 @@ __device__ __forceinline__ void cm_subgroup(M3<R>& u, const M3<R>& A, double bet
     // su2_to_quaternion (src/su3/utils.cpp:47-50)
     Quat w = {((double)wii.re + (double)wjj.re) / 2.0, ((double)wij.im + (double)wji.im) / 2.0,
               ((double)wij.re - (double)wji.re) / 2.0, ((double)wii.im - (double)wjj.im) / 2.0};
-    Quat r = su2_step(beta, w, rng, err);
+    Quat r = su2_step(c_alpha, w, rng, err);
     // su2_quaternion_to_su3 (src/su3/utils.cpp:33-44) applied from the left
     Cx<R> rii = mkc<R>((R)r.a0, (R)r.a3), rjj = mkc<R>((R)r.a0, (R)-r.a3);
     Cx<R> rij = mkc<R>((R)r.a2, (R)r.a1), rji = mkc<R>((R)-r.a2, (R)r.a1);
@@ -191,16 +191,14 @@ __device__ __forceinline__ void cm_subgroup(M3<R>& u, const M3<R>& A, double bet
     }
 }
 
-// Heatbath update of every link (x, MU) with parity(x) == par (one (parity, direction)
-// set of the checkerboard: no link of the set appears in another's staple, so all of them
-// update concurrently).  Replaces mpi::heatbathcb::sweep (heatbath_mpi.cpp:36-57) for one
-// (parity, mu); the staple is computed once per link, since it does not contain U(x,MU)
-// and is therefore identical for every hit (the reference recomputes it per hit).
+// Heatbath update of one link (x, mu) of the (parity, mu) set being swept: no link of the set
+// appears in another's staple, so all links of the set update concurrently.  Replaces
+// mpi::heatbathcb::hit / sweep (heatbath_mpi.cpp:10-57) for one link; the staple is computed
+// once per link, since it does not contain U(x,mu) and is therefore identical for every hit
+// (the reference recomputes it per hit).  MU >= 0 selects the direction at compile time.
 template <typename R, int NE, int MU>
-__global__ void __launch_bounds__(QCB_HB_THREADS, QCB_HB_MINB(R)) k_hb_subsweep(Geom g, LinkField<R, NE> U, int par, double beta, int n_hits,
-                                                      uint64_t seed, uint32_t sweep, int reproject, int* err) {
-    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= g.Vh) return;
+__device__ __forceinline__ void hb_link(const Geom& g, const LinkField<R, NE>& U, int par, int64_t h, double c_alpha,
+                                        int n_hits, uint64_t seed, uint32_t sweep, int reproject, int* err) {
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
     const int64_t lex = lex_of(g, c);
@@ -208,9 +206,9 @@ __global__ void __launch_bounds__(QCB_HB_THREADS, QCB_HB_MINB(R)) k_hb_subsweep(
     M3<R> u = U.load(MU, par, h);
     LinkStream rng(seed, (uint32_t)(lex * 4 + MU), sweep, TAG_HB);
     for (int hit = 0; hit < n_hits; hit++) {
-        cm_subgroup<R, 0, 1>(u, A, beta, rng, err);
-        cm_subgroup<R, 1, 2>(u, A, beta, rng, err);
-        cm_subgroup<R, 0, 2>(u, A, beta, rng, err);
+        cm_subgroup<R, 0, 1>(u, A, c_alpha, rng, err);
+        cm_subgroup<R, 1, 2>(u, A, c_alpha, rng, err);
+        cm_subgroup<R, 0, 2>(u, A, c_alpha, rng, err);
     }
     if (reproject) {
         M3<double> ud = convert<double>(u);
@@ -218,6 +216,17 @@ __global__ void __launch_bounds__(QCB_HB_THREADS, QCB_HB_MINB(R)) k_hb_subsweep(
         u = convert<R>(ud);
     }
     U.store(MU, par, h, u);
+}
+
+// Single-lattice heatbath launch: one thread per link of the (par, MU) set, geometry as kernel
+// parameters.
+template <typename R, int NE, int MU>
+__global__ void __launch_bounds__(QCB_HB_THREADS, QCB_HB_MINB(R))
+    k_hb_subsweep(Geom g, LinkField<R, NE> U, int par, double c_alpha, int n_hits, uint64_t seed, uint32_t sweep,
+                  int reproject, int* err) {
+    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= g.Vh) return;
+    hb_link<R, NE, MU>(g, U, par, h, c_alpha, n_hits, seed, sweep, reproject, err);
 }
 
 // ------------------------------------------------------------------ Wilson flow
@@ -283,16 +292,15 @@ __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>&
     Wout.store(mu, par, h, w);
 }
 
-// Grid: blockIdx.x = (site block) * 8 + (mu*2 + parity), so the 8 link classes of a block of
-// sites run together and share their neighbour links in L2.
+// Single-lattice RK3 stage.  Grid: blockIdx.x = (site block) * 8 + (mu*2 + parity), so the 8
+// link classes of a block of sites run together and share their neighbour links in L2.
 template <typename R, int NE, int STAGE>
 __global__ void __launch_bounds__(QCB_FLOW_THREADS, QCB_FLOW_MINB(R))
     k_flow_stage(Geom g, LinkField<R, NE> Win, LinkField<R, NE> Wout, AlgField<R> Z, double eps, int reproject) {
     const int lt = blockIdx.x & 7;
-    const int mu = lt >> 1, par = lt & 1;
     const int64_t h = (int64_t)(blockIdx.x >> 3) * blockDim.x + threadIdx.x;
     if (h >= g.Vh) return;
-    flow_link<R, NE, STAGE>(g, Win, Wout, Z, eps, mu, par, h, reproject);
+    flow_link<R, NE, STAGE>(g, Win, Wout, Z, eps, lt >> 1, lt & 1, h, reproject);
 }
 
 // ------------------------------------------------------------------ reductions
@@ -333,29 +341,35 @@ __global__ void k_finalize(const double* partials, int nb, int nv, unsigned max_
 
 // Plaquette (observables_mpi.cpp:11-35): per site sum over mu<nu of Re Tr(U_mu(x) U_nu(x+mu)
 // U_mu(x+nu)^dag U_nu(x)^dag)/3, evaluated as Re Tr((U_mu(x) U_nu(x+mu)) (U_nu(x) U_mu(x+nu))^dag).
+// Plaquette sum of one site: sum over mu<nu of Re Tr(U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag)/3
+// (observables_mpi.cpp:11-35), evaluated as Re Tr((U_mu(x) U_nu(x+mu)) (U_nu(x) U_mu(x+nu))^dag).
+template <typename R, int NE>
+__device__ __forceinline__ double site_plaquette(const Geom& g, const LinkField<R, NE>& U, int par, int64_t h) {
+    int c[4];
+    site_coords(g, par, (uint32_t)h, c);
+    const int64_t lex = lex_of(g, c);
+    double s = 0.0;
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+        const int64_t xmu = step_up(g, lex, c[mu], mu);
+        M3<R> umu = U.load_ro(mu, par, h);
+#pragma unroll
+        for (int nu = mu + 1; nu < 4; nu++) {
+            const int64_t xnu = step_up(g, lex, c[nu], nu);
+            M3<R> p1 = mul_nn(umu, U.load_ro(nu, par ^ 1, xmu >> 1));
+            M3<R> p2 = mul_nn(U.load_ro(nu, par, h), U.load_ro(mu, par ^ 1, xnu >> 1));
+            s += (double)re_tr_mul_na(p1, p2) / 3.0;
+        }
+    }
+    return s;
+}
+
 template <typename R, int NE>
 __global__ void __launch_bounds__(256) k_plaquette(Geom g, LinkField<R, NE> U, double* partials) {
     const int par = blockIdx.y;
     double v[1] = {0.0};
-    for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.x * blockDim.x) {
-        int c[4];
-        site_coords(g, par, (uint32_t)h, c);
-        const int64_t lex = lex_of(g, c);
-        double s = 0.0;
-#pragma unroll
-        for (int mu = 0; mu < 4; mu++) {
-            const int64_t xmu = step_up(g, lex, c[mu], mu);
-            M3<R> umu = U.load_ro(mu, par, h);
-#pragma unroll
-            for (int nu = mu + 1; nu < 4; nu++) {
-                const int64_t xnu = step_up(g, lex, c[nu], nu);
-                M3<R> p1 = mul_nn(umu, U.load_ro(nu, par ^ 1, xmu >> 1));
-                M3<R> p2 = mul_nn(U.load_ro(nu, par, h), U.load_ro(mu, par ^ 1, xnu >> 1));
-                s += (double)re_tr_mul_na(p1, p2) / 3.0;
-            }
-        }
-        v[0] += s;
-    }
+    for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.x * blockDim.x)
+        v[0] += site_plaquette(g, U, par, h);
     block_sum_store<1>(v, partials, blockIdx.y * gridDim.x + blockIdx.x);
 }
 
@@ -395,24 +409,30 @@ __device__ __forceinline__ M3<R> clover_F(const Geom& g, const LinkField<R, NE>&
     return F;
 }
 
-// local_q_e_clover (observables_mpi.cpp:93-112), one thread per (site, plane pair):
+// local_q_e_clover (observables_mpi.cpp:93-112) for one (site, plane pair):
 // pair 0: +Re Tr(F01 F23), pair 1: -Re Tr(F02 F13), pair 2: +Re Tr(F03 F12); e += |F|^2/2.
+// Adds (q/(4 pi^2), e) to v.
+template <typename R, int NE>
+__device__ __forceinline__ void site_clover_pair(const Geom& g, const LinkField<R, NE>& U, int par, int pair,
+                                                 int64_t h, double v[2]) {
+    const int a_mu = 0, a_nu = pair + 1;
+    const int b_mu = (pair == 0) ? 2 : 1, b_nu = (pair == 2) ? 2 : 3;
+    int c[4];
+    site_coords(g, par, (uint32_t)h, c);
+    const int64_t lex = lex_of(g, c);
+    M3<R> Fa = clover_F(g, U, c, lex, par, a_mu, a_nu);
+    M3<R> Fb = clover_F(g, U, c, lex, par, b_mu, b_nu);
+    double q = (double)re_tr_mul(Fa, Fb);
+    v[0] += (pair == 1 ? -q : q) * (1.0 / (4.0 * kPi * kPi));
+    v[1] += 0.5 * ((double)sq_norm(Fa) + (double)sq_norm(Fb));
+}
+
 template <typename R, int NE>
 __global__ void __launch_bounds__(128) k_clover_qe(Geom g, LinkField<R, NE> U, double* partials) {
     const int par = blockIdx.y & 1, pair = blockIdx.y >> 1;
-    const int a_mu = 0, a_nu = pair + 1;
-    const int b_mu = (pair == 0) ? 2 : 1, b_nu = (pair == 2) ? 2 : 3;
     double v[2] = {0.0, 0.0};
-    for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.x * blockDim.x) {
-        int c[4];
-        site_coords(g, par, (uint32_t)h, c);
-        const int64_t lex = lex_of(g, c);
-        M3<R> Fa = clover_F(g, U, c, lex, par, a_mu, a_nu);
-        M3<R> Fb = clover_F(g, U, c, lex, par, b_mu, b_nu);
-        double q = (double)re_tr_mul(Fa, Fb);
-        v[0] += (pair == 1 ? -q : q) * (1.0 / (4.0 * kPi * kPi));
-        v[1] += 0.5 * ((double)sq_norm(Fa) + (double)sq_norm(Fb));
-    }
+    for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.x * blockDim.x)
+        site_clover_pair(g, U, par, pair, h, v);
     block_sum_store<2>(v, partials, blockIdx.y * gridDim.x + blockIdx.x);
 }
 

@@ -41,6 +41,7 @@ extern "C" {
 
 typedef struct qcb_field_s* qcb_field;
 typedef struct qcb_flow_s* qcb_flow;
+typedef struct qcb_batch_s* qcb_batch;
 
 /* Message of the last failing call on this host thread ("" if none). */
 const char* qcb_last_error(void);
@@ -155,6 +156,38 @@ int qcb_diag_staple(qcb_field f, int mu, double* out);
 int qcb_diag_exp_su3(const double* Z, int n, double coeff, int prec, double* out);
 /* n Philox4x32-10 blocks on the device: ctr word 0 = ctr[0] + i. */
 int qcb_diag_philox(const uint32_t ctr[4], const uint32_t key[2], int n, uint32_t* out);
+
+/* ------------------------------------------------------------------ batched chains */
+/* Many independent heatbath chains (the reference runs one chain per MPI job: src/bin/gauge_hb_cb.cpp
+ * generate_hb_cb :20-247) advanced together on one GPU.  n lattices, extents L[4i..4i+3] (even,
+ * >= 2), couplings beta[i], stream seeds seed[i], one storage format; all links start cold.
+ * Chain i draws exactly what qcb_hb_sweep(field_i, beta[i], n_hits, seed[i], sweep) would for the
+ * batch's sweep counter (0, 1, 2, ...). */
+int qcb_batch_create(int n, const int* L, const double* beta, const uint64_t* seed, int prec, int store,
+                     qcb_batch* out);
+int qcb_batch_destroy(qcb_batch b);
+int qcb_batch_info(qcb_batch b, int* n, int* prec, int* store, int* variant, uint32_t* sweep);
+void* qcb_batch_stream(qcb_batch b);
+/* hot_start / cold_start of every chain (chain i as qcb_hot_start(field, seed[i])). */
+int qcb_batch_hot_start(qcb_batch b);
+int qcb_batch_cold_start(qcb_batch b);
+/* n_sweeps full sweeps of every chain.  Each (parity, mu) phase of all chains is one persistent
+ * launch over a tile work list; one sweep (8 phases + the device sweep counter) is captured as a
+ * CUDA graph at the first call with a given n_hits / launch shape and replayed. */
+int qcb_batch_sweep(qcb_batch b, int n_hits, int n_sweeps);
+/* Waits for queued work and reports a device-side heatbath error (QCB_ERANGE). */
+int qcb_batch_sync(qcb_batch b);
+/* Mean plaquette of every chain (out: n doubles). */
+int qcb_batch_plaquette(qcb_batch b, double* out);
+int qcb_batch_upload_aos(qcb_batch b, int i, const double* links);
+int qcb_batch_download_aos(qcb_batch b, int i, double* links);
+/* Launch shape of the heatbath phases (0: 64 threads, 1: 128, 2: 256 per block). */
+int qcb_batch_set_variant(qcb_batch b, int variant);
+/* Autotuner: times n_trial sweeps of every launch shape on the live batch (all shapes compute the
+ * same links, so these are ordinary sweeps of the chains) and keeps the fastest; with
+ * allow_store_change it also times the other link storage (18 <-> 12 reals) on a converted copy
+ * and adopts it if faster.  ms_out (may be NULL): 4 times per sweep (3 shapes, other storage). */
+int qcb_batch_tune(qcb_batch b, int n_hits, int n_trial, int allow_store_change, int* variant_out, double* ms_out);
 
 /* ------------------------------------------------------------------ allocation-free entry */
 /* No counterpart in the reference (its plaquette, observables_mpi.cpp:39-48, runs on host
