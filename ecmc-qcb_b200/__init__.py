@@ -96,6 +96,13 @@ def exported_symbols():
         "qcb_batch_download_aos": (i, [_vp, i, _vp]),
         "qcb_batch_set_variant": (i, [_vp, i]),
         "qcb_batch_tune": (i, [_vp, i, i, i, pi, pd]),
+        "qcb_serve_create": (i, [sz, i, i, i, i, C.POINTER(_vp)]),
+        "qcb_serve_destroy": (i, [_vp]),
+        "qcb_serve_now": (d, [_vp]),
+        "qcb_serve_submit": (i, [_vp, u64, _i4, _vp, d, i]),
+        "qcb_serve_poll": (i, [_vp, C.POINTER(u64), pd, i, pi, pd]),
+        "qcb_serve_wait": (i, [_vp, d]),
+        "qcb_serve_stats": (i, [_vp, pd]),
     }
 
 
@@ -331,6 +338,59 @@ class Batch:
         ms = (C.c_double * 4)()
         _check(lib().qcb_batch_tune(self.h, int(n_hits), int(n_trial), 1 if allow_store_change else 0, C.byref(v), ms))
         return v.value, list(ms)
+
+
+class Server:
+    """Continuous-batching flow-measurement server (its own scheduler thread in libqcb.so)."""
+
+    def __init__(self, budget_bytes: int, prec: int = PREC_F32, store: int = STORE_18, n_rk: int = 1,
+                 max_active: int = 0):
+        h = _vp()
+        _check(lib().qcb_serve_create(int(budget_bytes), int(prec), int(store), int(n_rk), int(max_active),
+                                      C.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().qcb_serve_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def now(self) -> float:
+        return lib().qcb_serve_now(self.h)
+
+    def submit(self, rid: int, L, U: np.ndarray, eps: float, n_steps: int) -> None:
+        U = np.ascontiguousarray(U, dtype=np.complex128)
+        _check(lib().qcb_serve_submit(self.h, int(rid), _i4(*[int(v) for v in L]), U.ctypes.data, float(eps),
+                                      int(n_steps)))
+
+    def poll(self, max_steps: int = 1 << 16):
+        """Returns (id, tQE (n,3), (t_submit, t_admit, t_done)) or None."""
+        rid = C.c_uint64()
+        buf = np.empty(3 * max_steps)
+        n = C.c_int()
+        t = (C.c_double * 3)()
+        r = lib().qcb_serve_poll(self.h, C.byref(rid), buf.ctypes.data_as(C.POINTER(C.c_double)), int(max_steps),
+                                 C.byref(n), t)
+        if r < 0:
+            _check(r)
+        if r == 0:
+            return None
+        return rid.value, buf[:3 * n.value].reshape(n.value, 3).copy(), tuple(t)
+
+    def wait(self, timeout_s: float = 600.0) -> None:
+        _check(lib().qcb_serve_wait(self.h, float(timeout_s)))
+
+    def stats(self):
+        o = (C.c_double * 8)()
+        _check(lib().qcb_serve_stats(self.h, o))
+        keys = ["submitted", "completed", "ticks", "peak_resident", "peak_bytes", "bytes_in_use", "busy_s", "queued"]
+        return dict(zip(keys, list(o)))
 
 
 def ildg_probe(path: str):

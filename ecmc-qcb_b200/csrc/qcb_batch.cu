@@ -309,7 +309,7 @@ int qcb_batch_sync(qcb_batch b) {
 int qcb_batch_plaquette(qcb_batch b, double* out) {
     if (!b || !out) return fail(QCB_EINVAL, "null argument");
     const WorkList w = batch_list(b);
-    CK(fmt_ops(b->fmt).plaq_tiles(w, 0, b->partials, b->stream));
+    CK(fmt_ops(b->fmt).plaq_tiles(w, -1, b->partials, b->stream));
     k_lat_finalize<<<b->n, 256, 0, b->stream>>>(b->d_desc, LatDesc{}, b->partials, 2, 1, 1, b->d_out);
     CK(cudaGetLastError());
     note_launches(2);

@@ -59,18 +59,18 @@ struct FmtImpl {
     }
 
     template <int STAGE>
-    static cudaError_t flow_launch(const WorkList& w, int rep, cudaStream_t s) {
+    static cudaError_t flow_launch(const WorkList& w, int flip_xor, int rep, cudaStream_t s) {
         static int cache = 0;
         auto k = k_flow_tiles<R, NE, STAGE>;
         const int ntiles = 8 * w.nb_total;
         const int grid = std::min(ntiles, resident_blocks(k, QCB_FLOW_THREADS, &cache));
-        k<<<grid, QCB_FLOW_THREADS, 0, s>>>(w.lats, w.tile_lat, w.one, ntiles, rep);
+        k<<<grid, QCB_FLOW_THREADS, 0, s>>>(w.lats, w.tile_lat, w.one, ntiles, flip_xor, rep);
         return cudaGetLastError();
     }
-    static cudaError_t flow(const WorkList& w, int stage, int rep, cudaStream_t s) {
-        if (stage == 1) return flow_launch<1>(w, rep, s);
-        if (stage == 2) return flow_launch<2>(w, rep, s);
-        return flow_launch<3>(w, rep, s);
+    static cudaError_t flow(const WorkList& w, int stage, int flip_xor, int rep, cudaStream_t s) {
+        if (stage == 1) return flow_launch<1>(w, flip_xor, rep, s);
+        if (stage == 2) return flow_launch<2>(w, flip_xor, rep, s);
+        return flow_launch<3>(w, flip_xor, rep, s);
     }
 
     template <int MU>
@@ -106,14 +106,14 @@ struct FmtImpl {
     }
 
     // Reduction work lists are not persistent: one block per tile, one partial per tile.
-    static cudaError_t plaq_tiles(const WorkList& w, int flow_current, double* partials, cudaStream_t s) {
+    static cudaError_t plaq_tiles(const WorkList& w, int flip_xor, double* partials, cudaStream_t s) {
         const int ntiles = 2 * w.nb_total;
-        k_plaq_tiles<R, NE><<<ntiles, TILE, 0, s>>>(w.lats, w.tile_lat, w.one, ntiles, flow_current, partials);
+        k_plaq_tiles<R, NE><<<ntiles, TILE, 0, s>>>(w.lats, w.tile_lat, w.one, ntiles, flip_xor, partials);
         return cudaGetLastError();
     }
-    static cudaError_t clover_tiles(const WorkList& w, int flow_current, double* partials, cudaStream_t s) {
+    static cudaError_t clover_tiles(const WorkList& w, int flip_xor, double* partials, cudaStream_t s) {
         const int ntiles = 6 * w.nb_total;
-        k_clover_tiles<R, NE><<<ntiles, TILE, 0, s>>>(w.lats, w.tile_lat, w.one, ntiles, flow_current, partials);
+        k_clover_tiles<R, NE><<<ntiles, TILE, 0, s>>>(w.lats, w.tile_lat, w.one, ntiles, flip_xor, partials);
         return cudaGetLastError();
     }
 

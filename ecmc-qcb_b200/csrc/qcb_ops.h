@@ -26,9 +26,9 @@ struct FmtOps {
     // ---- work-list kernels (one or many lattices)
     cudaError_t (*hb)(const WorkList& w, int variant, int par, int mu, int n_hits, const uint32_t* sweep_dev,
                       uint32_t sweep_add, int reproject, int* err, cudaStream_t s);
-    cudaError_t (*flow)(const WorkList& w, int stage, int reproject, cudaStream_t s);
-    cudaError_t (*plaq_tiles)(const WorkList& w, int flow_current, double* partials, cudaStream_t s);
-    cudaError_t (*clover_tiles)(const WorkList& w, int flow_current, double* partials, cudaStream_t s);
+    cudaError_t (*flow)(const WorkList& w, int stage, int flip_xor, int reproject, cudaStream_t s);
+    cudaError_t (*plaq_tiles)(const WorkList& w, int flip_xor, double* partials, cudaStream_t s);
+    cudaError_t (*clover_tiles)(const WorkList& w, int flip_xor, double* partials, cudaStream_t s);
     // ---- single-lattice kernels
     cudaError_t (*hb1)(const Geom& g, void* links, int par, int mu, double c_alpha, int n_hits, uint64_t seed,
                        uint32_t sweep, int reproject, int* err, cudaStream_t s);

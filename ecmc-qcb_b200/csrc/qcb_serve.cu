@@ -1,0 +1,450 @@
+// qcb_serve.cu -- continuous-batching Wilson-flow measurement server.
+//
+// Requests (a configuration of any L^4 size, a flow step, a number of measured steps) arrive
+// through qcb_serve_submit from any host thread.  A scheduler thread owns the GPU work:
+//   * admission: requests leave the FIFO in order as soon as the HBM budget (and the active
+//     limit) leaves room for their flowed field, RK3 buffers and measurements; memory comes from
+//     the server's own stream-ordered pool and returns to it when a request completes;
+//   * one scheduler tick measures Q/E of every resident request (one batched clover launch and
+//     one per-request finalize) and then advances every resident request by n_rk RK3 steps with
+//     three persistent launches per step over the tile work list of all of them, so requests
+//     that arrive while others are on the GPU share the same launches;
+//   * a request that has taken its last measurement is copied back, frees its memory and is
+//     handed to qcb_serve_poll with its submit and completion times.
+// Per-request results do not depend on the other requests in the mix: every link and every
+// per-request reduction is computed exactly as it would be alone.
+// Replaces the measurement loop of topo_charge_flowed (src/observables/observables_mpi.cpp:159-186)
+// driven once per configuration by the reference's drivers (src/bin/gauge_hb_cb.cpp:184-197).
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "qcb_internal.h"
+#include "qcb_ops.h"
+
+using namespace qcb;
+
+namespace {
+
+struct Request {
+    uint64_t id = 0;
+    Geom g{};
+    double eps = 0.02;
+    int n_steps = 1;
+    std::vector<double> input;  // host AoS FP64 links, dropped after upload
+    std::vector<double> tqe;    // 3 * n_steps results
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    void* buf = nullptr;  // W, W', Z, measurements in one allocation
+    size_t bytes = 0;
+    size_t off_out = 0, off_z = 0, off_meas = 0;
+    int tick0 = 0;
+    int flip = 0;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+struct qcb_server_s {
+    size_t budget = 0;
+    int prec = 32, store = 0, fmt = 2, max_active = 1 << 30, n_rk = 1;
+    int device = 0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request*> pending, done;
+    std::vector<Request*> active;
+    size_t bytes_in_use = 0, bytes_peak = 0;
+    uint64_t submitted = 0, completed = 0;
+    bool stop = false;
+    int err = QCB_OK;
+    std::string errmsg;
+    std::thread th;
+    cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+    // work list of the active set
+    std::vector<LatDesc> desc;
+    LatDesc* d_desc = nullptr;
+    size_t desc_cap = 0;
+    int* d_tile_lat = nullptr;
+    size_t tile_cap = 0;
+    int nb_total = 0;
+    double* partials = nullptr;
+    size_t partials_cap = 0;
+    double2* staging = nullptr;
+    size_t staging_cap = 0;
+    // counters
+    int tick = 0;       // measurements taken by the scheduler (slot index base)
+    uint64_t nflow = 0; // RK3 steps executed (buffer parity)
+    uint64_t ticks = 0;
+    int active_peak = 0;
+    double busy = 0.0;
+    std::chrono::steady_clock::time_point t0;
+    double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+};
+
+namespace {
+
+// Per-request deterministic sums of clover partials, stored in the request's slot of this tick:
+// meas[(tick - tick0) * 2 + k] = (Q, sum e).
+__global__ void k_meas_finalize(const LatDesc* __restrict__ lats, const double* __restrict__ partials, int tick) {
+    __shared__ double sm[256];
+    const LatDesc* d = lats + blockIdx.x;
+    const int t0 = 6 * d->nb_begin, nt = 6 * d->nb;
+    for (int k = 0; k < 2; k++) {
+        double acc = 0.0;
+        for (int i = threadIdx.x; i < nt; i += 256) acc += partials[(size_t)(t0 + i) * 2 + k];
+        sm[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = 128; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) d->meas[(size_t)(tick - d->tick0) * 2 + k] = sm[0];
+        __syncthreads();
+    }
+}
+
+int set_error(qcb_server_s* s, int code, const std::string& msg) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->err == QCB_OK) {
+        s->err = code;
+        s->errmsg = msg;
+    }
+    s->cv_done.notify_all();
+    return code;
+}
+
+bool cuda_ok(qcb_server_s* s, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    set_error(s, e == cudaErrorMemoryAllocation ? QCB_ENOMEM : QCB_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return false;
+}
+
+template <typename T>
+bool grow(qcb_server_s* s, T** p, size_t* cap, size_t n) {
+    if (*cap >= n) return true;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    size_t m = std::max<size_t>(n, 1024);
+    if (!cuda_ok(s, cudaMalloc((void**)p, m * sizeof(T)), "server work-list buffer")) return false;
+    *cap = m;
+    return true;
+}
+
+// Rebuilds the descriptors and tile map of the active set.
+bool rebuild(qcb_server_s* s) {
+    s->desc.clear();
+    std::vector<int> tile_lat;
+    int nb = 0;
+    for (size_t i = 0; i < s->active.size(); i++) {
+        Request* r = s->active[i];
+        LatDesc d;
+        memset(&d, 0, sizeof(d));
+        d.g = r->g;
+        d.links = r->buf;
+        d.links_out = (char*)r->buf + r->off_out;
+        d.z = (char*)r->buf + r->off_z;
+        d.meas = (double*)((char*)r->buf + r->off_meas);
+        d.eps = r->eps;
+        d.nb_begin = nb;
+        d.nb = (int)((r->g.Vh + TILE - 1) / TILE);
+        d.flip = r->flip;
+        d.tick0 = r->tick0;
+        for (int k = 0; k < d.nb; k++) tile_lat.push_back((int)i);
+        nb += d.nb;
+        s->desc.push_back(d);
+    }
+    s->nb_total = nb;
+    if (s->desc.empty()) return true;
+    if (!grow(s, &s->d_desc, &s->desc_cap, s->desc.size())) return false;
+    if (!grow(s, &s->d_tile_lat, &s->tile_cap, tile_lat.size())) return false;
+    if (!grow(s, &s->partials, &s->partials_cap, (size_t)12 * nb)) return false;
+    // pageable sources: the copies are staged before the calls return
+    if (!cuda_ok(s, cudaMemcpyAsync(s->d_desc, s->desc.data(), sizeof(LatDesc) * s->desc.size(),
+                                    cudaMemcpyHostToDevice, s->stream), "descriptor upload"))
+        return false;
+    return cuda_ok(s, cudaMemcpyAsync(s->d_tile_lat, tile_lat.data(), sizeof(int) * tile_lat.size(),
+                                      cudaMemcpyHostToDevice, s->stream), "tile map upload");
+}
+
+bool admit(qcb_server_s* s, Request* r) {
+    r->t_admit = s->now();
+    if (!cuda_ok(s, cudaMallocFromPoolAsync(&r->buf, r->bytes, s->pool, s->stream), "request allocation")) return false;
+    const size_t nd = (size_t)r->g.V * 72;
+    if (!grow(s, &s->staging, &s->staging_cap, nd / 2)) return false;
+    if (!cuda_ok(s, cudaMemcpyAsync(s->staging, r->input.data(), nd * sizeof(double), cudaMemcpyHostToDevice, s->stream),
+                 "request upload"))
+        return false;
+    if (!cuda_ok(s, fmt_ops(s->fmt).aos_to_soa(r->g, s->staging, r->buf, 0, s->stream), "request layout")) return false;
+    note_launches(1);
+    std::vector<double>().swap(r->input);
+    r->tick0 = s->tick;
+    r->flip = (int)(s->nflow & 1);  // current links in buffer A
+    return true;
+}
+
+bool finish(qcb_server_s* s, Request* r) {
+    std::vector<double> meas((size_t)r->n_steps * 2);
+    if (!cuda_ok(s, cudaMemcpyAsync(meas.data(), (char*)r->buf + r->off_meas, meas.size() * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s->stream), "result readback"))
+        return false;
+    if (!cuda_ok(s, cudaFreeAsync(r->buf, s->stream), "request free")) return false;
+    if (!cuda_ok(s, cudaStreamSynchronize(s->stream), "result sync")) return false;
+    r->buf = nullptr;
+    r->tqe.resize((size_t)r->n_steps * 3);
+    double t = 0.0;
+    for (int k = 0; k < r->n_steps; k++) {
+        r->tqe[3 * k] = t;
+        r->tqe[3 * k + 1] = meas[2 * k];
+        r->tqe[3 * k + 2] = meas[2 * k + 1] / (double)r->g.V;
+        for (int j = 0; j < s->n_rk; j++) t += r->eps;
+    }
+    r->t_done = s->now();
+    return true;
+}
+
+void scheduler(qcb_server_s* s) {
+    cudaSetDevice(s->device);
+    const int rep = (s->prec == QCB_PREC_F32) ? 1 : 0;
+    while (true) {
+        std::vector<Request*> fresh;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_work.wait(lk, [&] { return s->stop || !s->pending.empty() || !s->active.empty(); });
+            if (s->stop || s->err != QCB_OK) break;
+            while (!s->pending.empty() && (int)s->active.size() < s->max_active &&
+                   s->bytes_in_use + s->pending.front()->bytes <= s->budget) {
+                Request* r = s->pending.front();
+                s->pending.pop_front();
+                s->bytes_in_use += r->bytes;
+                s->bytes_peak = std::max(s->bytes_peak, s->bytes_in_use);
+                fresh.push_back(r);
+            }
+        }
+        const double tb = s->now();
+        bool ok = true;
+        for (Request* r : fresh) {
+            ok = ok && admit(s, r);
+            s->active.push_back(r);
+        }
+        if (ok && !fresh.empty()) ok = rebuild(s);
+        if (!ok) break;
+        if (s->active.empty()) continue;
+        // measure every resident request at its current step
+        WorkList w;
+        w.lats = s->d_desc;
+        w.tile_lat = s->d_tile_lat;
+        w.nb_total = s->nb_total;
+        w.nlat = (int)s->active.size();
+        const int fx = (int)(s->nflow & 1);
+        if (!cuda_ok(s, fmt_ops(s->fmt).clover_tiles(w, fx, s->partials, s->stream), "clover launch")) break;
+        k_meas_finalize<<<(unsigned)s->active.size(), 256, 0, s->stream>>>(s->d_desc, s->partials, s->tick);
+        if (!cuda_ok(s, cudaGetLastError(), "measure finalize")) break;
+        note_launches(2);
+        // requests that took their last measurement leave the mix
+        std::vector<Request*> leaving, staying;
+        for (Request* r : s->active) (s->tick - r->tick0 == r->n_steps - 1 ? leaving : staying).push_back(r);
+        s->tick++;
+        for (Request* r : leaving) ok = ok && finish(s, r);
+        if (!ok) break;
+        if (!leaving.empty()) {
+            s->active.swap(staying);
+            if (!rebuild(s)) break;
+            w.lats = s->d_desc;
+            w.tile_lat = s->d_tile_lat;
+            w.nb_total = s->nb_total;
+            w.nlat = (int)s->active.size();
+        }
+        for (int k = 0; k < s->n_rk && !s->active.empty() && ok; k++) {
+            const int f = (int)(s->nflow & 1);
+            for (int stage = 1; stage <= 3 && ok; stage++)
+                ok = cuda_ok(s, fmt_ops(s->fmt).flow(w, stage, f, rep, s->stream), "flow launch");
+            note_launches(3);
+            s->nflow++;
+        }
+        if (!ok) break;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->ticks++;
+            s->active_peak = std::max(s->active_peak, (int)s->active.size() + (int)leaving.size());
+            s->busy += s->now() - tb;
+            for (Request* r : leaving) {
+                s->bytes_in_use -= r->bytes;
+                s->done.push_back(r);
+                s->completed++;
+            }
+            if (!leaving.empty()) s->cv_done.notify_all();
+        }
+    }
+    cudaStreamSynchronize(s->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int qcb_serve_create(size_t hbm_budget_bytes, int prec, int store, int n_rk, int max_active, qcb_server* out) {
+    if (!out || hbm_budget_bytes == 0 || n_rk < 1) return fail(QCB_EINVAL, "serve: invalid argument");
+    if (prec != QCB_PREC_F64 && prec != QCB_PREC_F32) return fail(QCB_EINVAL, "prec must be 64 or 32");
+    if (store != QCB_STORE_18 && store != QCB_STORE_12) return fail(QCB_EINVAL, "store must be 0 or 1");
+    qcb_server_s* s = new (std::nothrow) qcb_server_s();
+    if (!s) return fail(QCB_ENOMEM, "host allocation");
+    s->budget = hbm_budget_bytes;
+    s->prec = prec;
+    s->store = store;
+    s->fmt = fmt_of(prec, store);
+    s->n_rk = n_rk;
+    s->max_active = max_active > 0 ? max_active : (1 << 30);
+    s->t0 = std::chrono::steady_clock::now();
+    cudaGetDevice(&s->device);
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = s->device;
+        e = cudaMemPoolCreate(&s->pool, &props);
+    }
+    if (e == cudaSuccess) {
+        uint64_t keep = hbm_budget_bytes;
+        e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    if (e != cudaSuccess) {
+        int r = fail(QCB_ECUDA, "serve create: %s", cudaGetErrorString(e));
+        qcb_serve_destroy(s);
+        return r;
+    }
+    s->th = std::thread(scheduler, s);
+    *out = s;
+    return QCB_OK;
+}
+
+int qcb_serve_destroy(qcb_server s) {
+    if (!s) return QCB_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->th.joinable()) s->th.join();
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (Request* r : s->active) {
+        if (r->buf) cudaFreeAsync(r->buf, s->stream);
+        delete r;
+    }
+    for (Request* r : s->pending) delete r;
+    for (Request* r : s->done) delete r;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->d_desc) cudaFree(s->d_desc);
+    if (s->d_tile_lat) cudaFree(s->d_tile_lat);
+    if (s->partials) cudaFree(s->partials);
+    if (s->staging) cudaFree(s->staging);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return QCB_OK;
+}
+
+double qcb_serve_now(qcb_server s) { return s ? s->now() : 0.0; }
+
+int qcb_serve_submit(qcb_server s, uint64_t id, const int L[4], const double* links, double eps, int n_steps) {
+    if (!s || !L || !links || !(eps > 0.0) || n_steps < 1) return fail(QCB_EINVAL, "serve submit: invalid argument");
+    int64_t V = 1;
+    for (int d = 0; d < 4; d++) {
+        if (L[d] < 2 || (L[d] & 1)) return fail(QCB_EINVAL, "serve submit: extents must be even and >= 2");
+        V *= L[d];
+    }
+    if (V > ((int64_t)1 << 30)) return fail(QCB_EINVAL, "serve submit: volume exceeds 2^30");
+    Request* r = new (std::nothrow) Request();
+    if (!r) return fail(QCB_ENOMEM, "host allocation");
+    r->id = id;
+    r->g = make_geom(L);
+    r->eps = eps;
+    r->n_steps = n_steps;
+    r->input.assign(links, links + (size_t)V * 72);
+    const size_t lb = align256(link_bytes(s->fmt, r->g.Vh));
+    r->off_out = lb;
+    r->off_z = 2 * lb;
+    r->off_meas = 2 * lb + align256(alg_bytes(s->fmt, r->g.Vh));
+    r->bytes = r->off_meas + align256((size_t)n_steps * 2 * sizeof(double));
+    if (r->bytes > s->budget) {
+        delete r;
+        return fail(QCB_ENOMEM, "serve submit: request needs %zu bytes, budget is %zu", r->bytes, s->budget);
+    }
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->err != QCB_OK) {
+            delete r;
+            return fail(s->err, "server stopped: %s", s->errmsg.c_str());
+        }
+        r->t_submit = s->now();
+        s->pending.push_back(r);
+        s->submitted++;
+    }
+    s->cv_work.notify_one();
+    return QCB_OK;
+}
+
+// Pops one completed request: returns 1 (and fills the outputs) or 0 if none is ready.
+// tQE must hold 3 * max_steps doubles; times are seconds on the server's clock.
+int qcb_serve_poll(qcb_server s, uint64_t* id, double* tQE, int max_steps, int* n_steps, double* times) {
+    if (!s) return fail(QCB_EINVAL, "null server");
+    Request* r = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->done.empty()) return s->err != QCB_OK ? fail(s->err, "server: %s", s->errmsg.c_str()) : 0;
+        r = s->done.front();
+        s->done.pop_front();
+    }
+    if (id) *id = r->id;
+    if (n_steps) *n_steps = r->n_steps;
+    if (tQE) memcpy(tQE, r->tqe.data(), sizeof(double) * 3 * std::min(max_steps, r->n_steps));
+    if (times) {
+        times[0] = r->t_submit;
+        times[1] = r->t_admit;
+        times[2] = r->t_done;
+    }
+    delete r;
+    return 1;
+}
+
+// Waits (bounded) until every submitted request has completed.
+int qcb_serve_wait(qcb_server s, double timeout_s) {
+    if (!s) return fail(QCB_EINVAL, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                                        [&] { return s->completed == s->submitted || s->err != QCB_OK; });
+    if (s->err != QCB_OK) return fail(s->err, "server: %s", s->errmsg.c_str());
+    if (!ok) return fail(QCB_ETIMEOUT, "serve wait: %llu of %llu requests done", (unsigned long long)s->completed,
+                         (unsigned long long)s->submitted);
+    return QCB_OK;
+}
+
+// stats: [0] submitted, [1] completed, [2] scheduler ticks, [3] peak resident requests,
+// [4] peak bytes in use, [5] bytes in use, [6] scheduler busy seconds, [7] queued requests.
+int qcb_serve_stats(qcb_server s, double* out) {
+    if (!s || !out) return fail(QCB_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    out[0] = (double)s->submitted;
+    out[1] = (double)s->completed;
+    out[2] = (double)s->ticks;
+    out[3] = (double)s->active_peak;
+    out[4] = (double)s->bytes_peak;
+    out[5] = (double)s->bytes_in_use;
+    out[6] = s->busy;
+    out[7] = (double)s->pending.size();
+    return QCB_OK;
+}
+
+}  // extern "C"

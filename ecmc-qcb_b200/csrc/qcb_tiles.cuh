@@ -18,13 +18,14 @@ struct LatDesc {
     void* links;      // heatbath: links updated in place; flow: buffer A of the ping-pong pair
     void* links_out;  // flow: buffer B of the ping-pong pair
     void* z;          // flow: su(3) accumulator (8 reals per link)
+    double* meas;     // serving: per-step measurements (nv doubles per step)
     double c_alpha;   // heatbath: -0.75 / beta
     double eps;       // flow step size
     uint64_t seed;    // heatbath stream key
     int nb_begin;     // prefix sum of the nb of the lattices before this one
     int nb;           // ceil(Vh / TILE)
-    int flip;         // flow: 1 if the current links sit in links_out
-    int pad;
+    int flip;         // flow: 1 if the current links sit in links_out (xor the launch's flip_xor)
+    int tick0;        // serving: scheduler tick at which this lattice took its first measurement
 };
 
 template <typename R, int NE>
@@ -65,11 +66,12 @@ __global__ void __launch_bounds__(BLOCK, MINB)
 
 // ---------------------------------------------------------------- flow, one RK3 stage
 // Tile classes interleave the 8 (mu, parity) link classes of a block of sites so that they
-// share their neighbour links in L2.  Input of stage s is links when (flip + s - 1) is even.
+// share their neighbour links in L2.  With f = flip ^ flip_xor, the input of stage s is links
+// when (f + s - 1) is even; a whole RK3 step therefore moves the field to the other buffer.
 template <typename R, int NE, int STAGE>
 __global__ void __launch_bounds__(QCB_FLOW_THREADS, QCB_FLOW_MINB(R))
     k_flow_tiles(const LatDesc* __restrict__ lats, const int* __restrict__ tile_lat, const LatDesc one, int ntiles,
-                 int reproject) {
+                 int flip_xor, int reproject) {
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const LatDesc* d = lattice_of(lats, tile_lat, one, t >> 3);
         const Geom g = d->g;
@@ -77,7 +79,7 @@ __global__ void __launch_bounds__(QCB_FLOW_THREADS, QCB_FLOW_MINB(R))
         const int cls = lt & 7;
         const int64_t h = (int64_t)(lt >> 3) * TILE + threadIdx.x;
         if (h >= g.Vh) continue;
-        const bool in_b = ((d->flip + STAGE - 1) & 1) != 0;
+        const bool in_b = (((d->flip ^ flip_xor) + STAGE - 1) & 1) != 0;
         const LinkField<R, NE> win = lview<R, NE>(in_b ? d->links_out : d->links, g.Vh);
         const LinkField<R, NE> wout = lview<R, NE>(in_b ? d->links : d->links_out, g.Vh);
         AlgField<R> z;
@@ -88,18 +90,19 @@ __global__ void __launch_bounds__(QCB_FLOW_THREADS, QCB_FLOW_MINB(R))
 }
 
 // ---------------------------------------------------------------- per-tile reductions
+// flip_xor < 0: measure `links`; otherwise measure the flow's current buffer (as above).
 // Plaquette: 2 tiles per block (one per parity); one partial per tile.
 template <typename R, int NE>
 __global__ void __launch_bounds__(TILE)
     k_plaq_tiles(const LatDesc* __restrict__ lats, const int* __restrict__ tile_lat, const LatDesc one, int ntiles,
-                 int flow_current, double* partials) {
+                 int flip_xor, double* partials) {
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const LatDesc* d = lattice_of(lats, tile_lat, one, t >> 1);
         const Geom g = d->g;
         const int lt = t - 2 * d->nb_begin;
         const int par = lt & 1;
         const int64_t h = (int64_t)(lt >> 1) * TILE + threadIdx.x;
-        void* base = (flow_current && d->flip) ? d->links_out : d->links;
+        void* base = (flip_xor >= 0 && (d->flip ^ flip_xor)) ? d->links_out : d->links;
         double v[1] = {h < g.Vh ? site_plaquette(g, lview<R, NE>(base, g.Vh), par, h) : 0.0};
         block_sum_store<1>(v, partials, t);
         __syncthreads();
@@ -110,14 +113,14 @@ __global__ void __launch_bounds__(TILE)
 template <typename R, int NE>
 __global__ void __launch_bounds__(TILE)
     k_clover_tiles(const LatDesc* __restrict__ lats, const int* __restrict__ tile_lat, const LatDesc one, int ntiles,
-                   int flow_current, double* partials) {
+                   int flip_xor, double* partials) {
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const LatDesc* d = lattice_of(lats, tile_lat, one, t / 6);
         const Geom g = d->g;
         const int lt = t - 6 * d->nb_begin;
         const int cls = lt % 6;
         const int64_t h = (int64_t)(lt / 6) * TILE + threadIdx.x;
-        void* base = (flow_current && d->flip) ? d->links_out : d->links;
+        void* base = (flip_xor >= 0 && (d->flip ^ flip_xor)) ? d->links_out : d->links;
         double v[2] = {0.0, 0.0};
         if (h < g.Vh) site_clover_pair(g, lview<R, NE>(base, g.Vh), cls & 1, cls >> 1, h, v);
         block_sum_store<2>(v, partials, t);

@@ -42,6 +42,7 @@ extern "C" {
 typedef struct qcb_field_s* qcb_field;
 typedef struct qcb_flow_s* qcb_flow;
 typedef struct qcb_batch_s* qcb_batch;
+typedef struct qcb_server_s* qcb_server;
 
 /* Message of the last failing call on this host thread ("" if none). */
 const char* qcb_last_error(void);
@@ -188,6 +189,27 @@ int qcb_batch_set_variant(qcb_batch b, int variant);
  * allow_store_change it also times the other link storage (18 <-> 12 reals) on a converted copy
  * and adopts it if faster.  ms_out (may be NULL): 4 times per sweep (3 shapes, other storage). */
 int qcb_batch_tune(qcb_batch b, int n_hits, int n_trial, int allow_store_change, int* variant_out, double* ms_out);
+
+/* ------------------------------------------------------------------ flow-measurement server */
+/* Continuous-batching service for topo_charge_flowed (src/observables/observables_mpi.cpp:159-186):
+ * requests of any lattice size are queued, admitted in order as the HBM budget allows, and every
+ * scheduler tick measures (Q, E) of all resident requests and advances them by n_rk RK3 steps in
+ * shared persistent launches.  Runs its own scheduler thread on the current device.
+ * max_active <= 0: no limit besides the budget. */
+int qcb_serve_create(size_t hbm_budget_bytes, int prec, int store, int n_rk, int max_active, qcb_server* out);
+int qcb_serve_destroy(qcb_server s);
+/* Seconds on the server's clock (the clock of the times returned by qcb_serve_poll). */
+double qcb_serve_now(qcb_server s);
+/* Queues one request (thread-safe): host AoS FP64 links of an L[0..3] lattice, flow step eps,
+ * n_steps measurements at t = 0, n_rk*eps, ... (n_steps - 1 flow blocks).  The links are copied. */
+int qcb_serve_submit(qcb_server s, uint64_t id, const int L[4], const double* links, double eps, int n_steps);
+/* Pops one completed request: returns 1 and fills id, tQE (3 * min(max_steps, n_steps) doubles:
+ * t, Q, E), n_steps and times[3] = (submitted, admitted, completed); returns 0 if none is ready. */
+int qcb_serve_poll(qcb_server s, uint64_t* id, double* tQE, int max_steps, int* n_steps, double* times);
+/* Waits at most timeout_s seconds for every submitted request to complete (QCB_ETIMEOUT otherwise). */
+int qcb_serve_wait(qcb_server s, double timeout_s);
+/* out[8]: submitted, completed, ticks, peak resident, peak bytes, bytes in use, busy s, queued. */
+int qcb_serve_stats(qcb_server s, double* out);
 
 /* ------------------------------------------------------------------ allocation-free entry */
 /* No counterpart in the reference (its plaquette, observables_mpi.cpp:39-48, runs on host
