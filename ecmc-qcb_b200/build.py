@@ -17,6 +17,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libqcb.so")
+HOST = os.path.join(HERE, "host", "src")
+COMPAT = os.path.join(HERE, "libqcb_compat.a")
+DRIVER = os.path.join(HERE, "qcb_hb_cb")
+CXX = "/usr/bin/g++"
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -55,7 +59,34 @@ def build(verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_host()
     return LIB
+
+
+def build_host() -> None:
+    """The C++ layer with the reference's signatures (libqcb_compat.a) and the run driver."""
+    srcs = [os.path.join(HOST, "qcb_compat.cpp"), os.path.join(HOST, "io", "io.cpp")]
+    objs = []
+    for src in srcs:
+        obj = os.path.join(BUILD, "host_" + os.path.basename(src).replace(".cpp", ".o"))
+        hdr = max(os.path.getmtime(h) for h in glob.glob(os.path.join(HOST, "**", "*.h"), recursive=True))
+        if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src), hdr):
+            r = subprocess.run([CXX, "-std=c++17", "-O2", "-fPIC", "-Wall", "-Wextra", "-c", src, "-o", obj],
+                               capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"g++ failed on {src}:\n{r.stderr}")
+        objs.append(obj)
+    if not os.path.exists(COMPAT) or os.path.getmtime(COMPAT) < max(os.path.getmtime(o) for o in objs):
+        if os.path.exists(COMPAT):
+            os.remove(COMPAT)
+        subprocess.run(["ar", "rcs", COMPAT, *objs], check=True)
+    drv = os.path.join(HOST, "bin", "gauge_hb_cb.cpp")
+    if not os.path.exists(DRIVER) or os.path.getmtime(DRIVER) < max(os.path.getmtime(drv), os.path.getmtime(COMPAT),
+                                                                   os.path.getmtime(LIB)):
+        r = subprocess.run([CXX, "-std=c++17", "-O2", "-Wall", "-Wextra", drv, COMPAT, "-L" + HERE, "-lqcb",
+                            "-Wl,-rpath,$ORIGIN", "-o", DRIVER], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"driver link failed:\n{r.stderr}")
 
 
 if __name__ == "__main__":
