@@ -99,14 +99,21 @@ class Clocks:
         try:
             self.f = tempfile.TemporaryFile(mode="w+")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
+            # the timed region starts once the sampler has produced its first line
+            t0 = time.time()
+            while time.time() - t0 < 5.0:
+                if os.fstat(self.f.fileno()).st_size > 0:
+                    break
+                time.sleep(0.02)
         except OSError:
             self.proc = None
         return self
 
     def __exit__(self, *a):
         if self.proc is not None:
+            time.sleep(0.05)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -263,6 +270,110 @@ def flow_accuracy(qcb, src, n_steps):
     return out
 
 
+def run_batch(qcb):
+    """Batched chains: 96x8^4 + 96x12^4 + 48x16^4 + 16x24^4, beta ~ U[5.7, 6.3], seeds 0..255, hot
+    starts, FP64; autotuned, CUDA-graph sweeps; against the same sweeps run chain by chain."""
+    import numpy as np
+    import torch
+
+    rng = np.random.default_rng(0)
+    Ls = [(8,) * 4] * 96 + [(12,) * 4] * 96 + [(16,) * 4] * 48 + [(24,) * 4] * 16
+    betas = rng.uniform(5.7, 6.3, len(Ls))
+    b = qcb.Batch(Ls, betas, list(range(len(Ls))))
+    b.hot_start()
+    variant, tune_ms = b.tune(1, 2, allow_store_change=True)
+    b.sweep(1, 2)
+    b.sync()
+    s = torch.cuda.ExternalStream(b.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_sw = 20
+    e0.record(s)
+    b.sweep(1, n_sw)
+    e1.record(s)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / n_sw
+    info = b.info()
+    b.close()
+    V = sum(L[0] ** 4 for L in Ls)
+    serial = 0.0
+    per = {}
+    for Lc, cnt in (((8,) * 4, 96), ((12,) * 4, 96), ((16,) * 4, 48), ((24,) * 4, 16)):
+        f = qcb.GaugeField(Lc)
+        f.hot_start(1)
+        for k in range(3):
+            f.hb_sweep(6.0, 1, 1, k)
+        f.sync()
+        t0 = time.perf_counter()
+        for k in range(10):
+            f.hb_sweep(6.0, 1, 1, 3 + k)
+        f.sync()
+        one = (time.perf_counter() - t0) / 10 * 1e3
+        per[f"{Lc[0]}^4"] = one
+        serial += cnt * one
+        f.close()
+    return {"chains": len(Ls), "sites": V, "n_hits": 1, "ms_per_sweep": ms, "link_upd_per_s": 4 * V / (ms * 1e-3),
+            "serial_ms_per_sweep": serial, "serial_single_sweep_ms": per, "speedup_vs_serial": serial / ms,
+            "tuned": {"variant": variant, "store": "12" if info["store"] == 1 else "18", "ms": tune_ms},
+            "launches_per_sweep": 9, "graph": True}
+
+
+def run_serve(qcb, n_req: int):
+    """Serving: Poisson arrivals at 100 req/s, L in {8,12,16,20,24,32} with p = (.3,.25,.2,.1,.1,.05),
+    beta ~ U[5.8, 6.3], inputs = 50 FP64 sweeps from seed = request id (excluded from latency), flow
+    eps = 0.02 to t = L^2/32 in FP32 with Q/E every step; against one-at-a-time plain FP64 flow."""
+    import numpy as np
+
+    rng = np.random.default_rng(2026)
+    sizes = rng.choice([8, 12, 16, 20, 24, 32], size=n_req, p=[.3, .25, .2, .1, .1, .05])
+    betas = rng.uniform(5.8, 6.3, n_req)
+    arr = np.cumsum(rng.exponential(1.0 / 100.0, n_req))
+    b = qcb.Batch([(int(x),) * 4 for x in sizes], betas, list(range(n_req)))
+    b.hot_start()
+    b.sweep(1, 50)
+    inputs = [b.download(i) for i in range(n_req)]
+    b.close()
+    steps = [int(round(x * x / 32 / 0.02)) + 1 for x in sizes]
+    site_steps = sum(int(x) ** 4 * (n - 1) for x, n in zip(sizes, steps))
+    srv = qcb.Server(150 << 30, prec=qcb.PREC_F32, store=qcb.STORE_18)
+    start = srv.now()
+    k, done = 0, {}
+    while len(done) < n_req:
+        now = srv.now() - start
+        while k < n_req and arr[k] <= now:
+            srv.submit(k, (int(sizes[k]),) * 4, inputs[k], 0.02, steps[k])
+            k += 1
+        r = srv.poll()
+        if r is None:
+            time.sleep(0.0005)
+            continue
+        done[r[0]] = r
+    lat = np.array([done[i][2][2] - (start + arr[i]) for i in range(n_req)])
+    wall = max(done[i][2][2] for i in range(n_req)) - start
+    st = srv.stats()
+    srv.close()
+    tq, lat2, busy = 0.0, [], 0.0
+    for i in range(n_req):
+        f = qcb.GaugeField((int(sizes[i]),) * 4, 64, 0)
+        f.upload(inputs[i])
+        fl = qcb.GradientFlow(f, 0.02, prec=64, store=0)
+        t0 = time.perf_counter()
+        fl.measure(f, steps[i], 1)
+        dt = time.perf_counter() - t0
+        busy += dt
+        tq = max(tq, arr[i]) + dt
+        lat2.append(tq - arr[i])
+        fl.close()
+        f.close()
+    lat2 = np.array(lat2)
+    return {"requests": n_req, "rate_per_s": 100.0, "site_steps": site_steps, "prec": "fp32-18",
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "configs_per_s": n_req / wall, "site_steps_per_s": site_steps / wall,
+            "peak_resident": st["peak_resident"], "peak_bytes": st["peak_bytes"],
+            "serial_fp64": {"p50_s": float(np.percentile(lat2, 50)), "p99_s": float(np.percentile(lat2, 99)),
+                            "configs_per_s": n_req / tq, "site_steps_per_s": site_steps / busy},
+            "speedup_configs_per_s": (n_req / wall) / (n_req / tq)}
+
+
 def run_ours(args, rank: int, world: int, local: int):
     import torch
 
@@ -348,6 +459,28 @@ def run_ours(args, rank: int, world: int, local: int):
         flow[k].update(acc[k])
         flow[k]["speedup_vs_fp64"] = flow[k]["site_steps_per_s"] / flow["fp64"]["site_steps_per_s"]
 
+    # ---------------- heatbath variants on the same lattice: N_hits = 1, FP32 links
+    hb_more = {}
+    for tag, prec, nh in (("fp64_nhits1", 64, 1), ("fp32_nhits2", 32, 2)):
+        g = qcb.GaugeField(L, prec, qcb.STORE_18)
+        g.copy_from(f)
+        for i in range(2):
+            g.hb_sweep(BETA, nh, SEED_HB, 50_000 + i)
+        g.timing(True)
+        g.timing_reset()
+        for i in range(5):
+            g.hb_sweep(BETA, nh, SEED_HB, 50_100 + i)
+        n, kms = g.timing_read(qcb.K_HB)
+        su = S_U[prec]
+        ach = 9 * su * (V // 2) / (kms / n * 1e-3) / 1e9
+        hb_more[tag] = {"link_upd_per_s": (V // 2) / (kms / n * 1e-3), "per_launch_ms": kms / n,
+                        "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                                     "frac": ach / hbm_peak}}
+        g.close()
+
+    batch = run_batch(qcb) if args.parts in ("all",) else None
+    serve = run_serve(qcb, args.serve_requests) if args.parts in ("all",) else None
+
     cpu = None
     if rank == 0 and args.cpu_seconds > 0:
         orc = load_oracle()
@@ -373,7 +506,10 @@ def run_ours(args, rank: int, world: int, local: int):
             "gpu_launches": n_launch,
             "clocks": clk.summary(),
             "plaquette_after": plaq,
+            "hb": hb_more,
             "flow": flow,
+            "batch": batch,
+            "serve": serve,
         }
         print(json.dumps(line), flush=True)
     f.close()
@@ -382,13 +518,16 @@ def run_ours(args, rank: int, world: int, local: int):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="length of the CPU-baseline sample (0 skips it)")
     ap.add_argument("--only", default="all", choices=["all", "hb", "flow"],
                     help="run one part (used for ncu captures of a single kernel family)")
+    ap.add_argument("--parts", default="all", choices=["all", "core"],
+                    help="core: skip the batch and serving sections")
+    ap.add_argument("--serve-requests", type=int, default=32)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

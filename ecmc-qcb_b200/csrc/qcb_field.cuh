@@ -6,14 +6,17 @@
 // neighbour table and frozen-link mask are replaced by periodic coordinate arithmetic on a
 // single periodic lattice: one GPU holds the whole lattice, so there is no halo to refresh.
 //
-// HBM layout of one field ("parity-split structure of arrays"):
-//     plane(mu, parity, e) = (mu*2 + parity)*NE + e,        e = 3*row + col
-//     element = base[ plane * Vh + h ]                       (one complex per element)
-// where h = lex/2 is the half-site index inside its parity (Lx is even, so the two sites
-// 2k, 2k+1 of an x-row have opposite parity and share h = k).  Consecutive threads own
-// consecutive h, so every element load is a fully coalesced 16-byte (FP64) or 8-byte
-// (FP32) access.  NE = 9 stores the full matrix (18 reals); NE = 6 stores the first two
-// rows (12 reals) and rebuilds the third in registers as conj(row0 x row1).
+// HBM layout of one field ("parity-split, tiled structure of arrays"):
+//     plane(mu, parity) = mu*2 + parity, tile = h / 32, lane = h % 32  (h = lex/2)
+//     element e of link (mu, parity, h) = base[((plane * nT + tile) * NE + e) * 32 + lane]
+// with one complex per element and nT = ceil(V/2 / 32).  Lx is even, so the two sites 2k, 2k+1
+// of an x-row have opposite parity and share h = k.  A warp of 32 consecutive h reads 32
+// consecutive complexes for every element (fully coalesced 16-byte FP64 / 8-byte FP32 accesses),
+// and the NE elements of one link sit at compile-time offsets e*32 from one base address, so a
+// link load costs one address computation.  NE = 9 stores the full matrix (18 reals); NE = 6 the
+// first two rows (12 reals), the third rebuilt in registers as conj(row0 x row1).
+// The untiled variant (TILED = false: element e at base[(plane*NE + e)*V/2 + h]) is the layout of
+// caller-owned links handed to the allocation-free entry point.
 #pragma once
 #include <stdint.h>
 
@@ -32,10 +35,42 @@ struct V2<float> {
     using T = float2;
 };
 
+// Division of 32-bit unsigned integers by an invariant divisor d (Granlund & Montgomery, "Division
+// by invariant integers using multiplication", PLDI 1994): q = (t + ((n - t) >> 1)) >> (l - 1),
+// t = mulhi(n, m), l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1; d = 1 returns n.
+struct FastDiv {
+    uint32_t d, m, s;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+    FastDiv f;
+    f.d = d;
+    if (d <= 1) {
+        f.m = 0;
+        f.s = 0;
+        return f;
+    }
+    uint32_t l = 0;
+    while ((1ull << l) < d) l++;
+    f.m = (uint32_t)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+    f.s = l;
+    return f;
+}
+QCB_HD uint32_t fdiv(uint32_t n, const FastDiv& f) {
+    if (f.d <= 1) return n;
+#ifdef __CUDA_ARCH__
+    const uint32_t t = __umulhi(n, f.m);
+#else
+    const uint32_t t = (uint32_t)(((uint64_t)n * f.m) >> 32);
+#endif
+    return (t + ((n - t) >> 1)) >> (f.s - 1);
+}
+
 struct Geom {
     int L[4];
     int stride[4];  // lexicographic strides (1, Lx, Lx*Ly, Lx*Ly*Lz)
+    FastDiv div[3];  // division by L[0], L[1], L[2]
     int64_t V, Vh;
+    int nT;  // 32-site tiles per parity: ceil(Vh / 32)
 };
 
 inline Geom make_geom(const int L[4]) {
@@ -45,25 +80,27 @@ inline Geom make_geom(const int L[4]) {
     g.stride[1] = L[0];
     g.stride[2] = L[0] * L[1];
     g.stride[3] = L[0] * L[1] * L[2];
+    for (int d = 0; d < 3; d++) g.div[d] = make_fastdiv((uint32_t)L[d]);
     g.V = (int64_t)L[0] * L[1] * L[2] * L[3];
     g.Vh = g.V / 2;
+    g.nT = (int)((g.Vh + 31) / 32);
     return g;
 }
 
-// Coordinates of half-site h of the given parity.
+// Coordinates of half-site h of the given parity (lexicographic index 2h or 2h+1; V <= 2^30).
 QCB_HD void site_coords(const Geom& g, int par, uint32_t h, int c[4]) {
-    uint32_t i = 2u * h;
-    uint32_t L0 = g.L[0], L1 = g.L[1], L2 = g.L[2];
-    c[0] = (int)(i % L0);
-    i /= L0;
-    c[1] = (int)(i % L1);
-    i /= L1;
-    c[2] = (int)(i % L2);
-    c[3] = (int)(i / L2);
+    const uint32_t i = 2u * h;
+    const uint32_t q0 = fdiv(i, g.div[0]);
+    const uint32_t q1 = fdiv(q0, g.div[1]);
+    const uint32_t q2 = fdiv(q1, g.div[2]);
+    c[0] = (int)(i - q0 * (uint32_t)g.L[0]);
+    c[1] = (int)(q0 - q1 * (uint32_t)g.L[1]);
+    c[2] = (int)(q1 - q2 * (uint32_t)g.L[2]);
+    c[3] = (int)q2;
     c[0] += (c[1] + c[2] + c[3] + par) & 1;
 }
-QCB_HD int64_t lex_of(const Geom& g, const int c[4]) {
-    return (int64_t)c[0] + (int64_t)c[1] * g.stride[1] + (int64_t)c[2] * g.stride[2] + (int64_t)c[3] * g.stride[3];
+QCB_HD int lex_of(const Geom& g, const int c[4]) {
+    return c[0] + c[1] * g.stride[1] + c[2] * g.stride[2] + c[3] * g.stride[3];
 }
 QCB_HD void lex_coords(const Geom& g, int64_t lex, int c[4]) {
     c[0] = (int)(lex % g.L[0]);
@@ -74,66 +111,86 @@ QCB_HD void lex_coords(const Geom& g, int64_t lex, int c[4]) {
     c[3] = (int)(lex / g.L[2]);
 }
 // lex index of the site one step up / down in direction d from a site with coordinate cd.
-QCB_HD int64_t step_up(const Geom& g, int64_t lex, int cd, int d) {
-    return (cd == g.L[d] - 1) ? lex - (int64_t)(g.L[d] - 1) * g.stride[d] : lex + g.stride[d];
+QCB_HD int step_up(const Geom& g, int lex, int cd, int d) {
+    return (cd == g.L[d] - 1) ? lex - (g.L[d] - 1) * g.stride[d] : lex + g.stride[d];
 }
-QCB_HD int64_t step_dn(const Geom& g, int64_t lex, int cd, int d) {
-    return (cd == 0) ? lex + (int64_t)(g.L[d] - 1) * g.stride[d] : lex - g.stride[d];
+QCB_HD int step_dn(const Geom& g, int lex, int cd, int d) {
+    return (cd == 0) ? lex + (g.L[d] - 1) * g.stride[d] : lex - g.stride[d];
 }
 
 // Link storage view; NE = 9 (18 reals) or 6 (12 reals, third row rebuilt on load).
-template <typename R, int NE>
+template <typename R, int NE, bool TILED = true>
 struct LinkField {
     typedef typename V2<R>::T C2;
     C2* p;
     int64_t Vh;
-    QCB_HD size_t plane(int mu, int par, int e) const { return (size_t)((mu * 2 + par) * NE + e) * (size_t)Vh; }
-    __device__ __forceinline__ M3<R> load(int mu, int par, int64_t h) const {
+    // index of element 0 of link (mu, par, h); element e is at +e * ES
+    static constexpr int64_t kTiledStride = 32;
+    QCB_HD int64_t es() const { return TILED ? kTiledStride : Vh; }
+    QCB_HD size_t index0(int mu, int par, int h) const {
+        if (TILED) {
+            const int nT = (int)((Vh + 31) >> 5);
+            const int tile = (mu * 2 + par) * nT + (h >> 5);
+            return (size_t)tile * (NE * 32) + (h & 31);
+        }
+        return (size_t)((mu * 2 + par) * NE) * (size_t)Vh + (size_t)h;
+    }
+    __device__ __forceinline__ M3<R> load(int mu, int par, int h) const {
         M3<R> u;
-        const C2* b = p + plane(mu, par, 0) + h;
+        const C2* b = p + index0(mu, par, h);
 #pragma unroll
         for (int e = 0; e < NE; e++) {
-            C2 v = b[(size_t)e * Vh];
+            C2 v = b[e * es()];
             u.e[e] = mkc<R>(v.x, v.y);
         }
         if (NE == 6) rebuild_row2(u);
         return u;
     }
     // read-only path for links that no thread of the running kernel writes
-    __device__ __forceinline__ M3<R> load_ro(int mu, int par, int64_t h) const {
+    __device__ __forceinline__ M3<R> load_ro(int mu, int par, int h) const {
         M3<R> u;
-        const C2* b = p + plane(mu, par, 0) + h;
+        const C2* b = p + index0(mu, par, h);
 #pragma unroll
         for (int e = 0; e < NE; e++) {
-            C2 v = __ldg(b + (size_t)e * Vh);
+            C2 v = __ldg(b + e * es());
             u.e[e] = mkc<R>(v.x, v.y);
         }
         if (NE == 6) rebuild_row2(u);
         return u;
     }
-    __device__ __forceinline__ void store(int mu, int par, int64_t h, const M3<R>& u) const {
-        C2* b = p + plane(mu, par, 0) + h;
+    __device__ __forceinline__ void store(int mu, int par, int h, const M3<R>& u) const {
+        C2* b = p + index0(mu, par, h);
 #pragma unroll
         for (int e = 0; e < NE; e++) {
             C2 v;
             v.x = u.e[e].re;
             v.y = u.e[e].im;
-            b[(size_t)e * Vh] = v;
+            b[e * es()] = v;
         }
+    }
+    // raw element copy of one link (no rebuild / re-encode for NE == 6)
+    __device__ __forceinline__ void copy_from(int mu, int par, int h, const LinkField& src, int spar, int sh) const {
+        C2* b = p + index0(mu, par, h);
+        const C2* a = src.p + src.index0(mu, spar, sh);
+#pragma unroll
+        for (int e = 0; e < NE; e++) b[e * es()] = __ldg(a + e * src.es());
     }
 };
 
-// su(3) algebra storage: 8 reals per link as 4 complex planes
+// su(3) algebra storage: 8 reals per link as 4 complex entries in the tiled layout above
 //   0: Z01, 1: Z02, 2: Z12, 3: (Im Z00, Im Z11);  Z22 = -i(Im Z00 + Im Z11), Zji = -conj(Zij).
 template <typename R>
 struct AlgField {
     typedef typename V2<R>::T C2;
     C2* p;
     int64_t Vh;
-    QCB_HD size_t plane(int mu, int par, int e) const { return (size_t)((mu * 2 + par) * 4 + e) * (size_t)Vh; }
-    __device__ __forceinline__ M3<R> load(int mu, int par, int64_t h) const {
-        const C2* b = p + plane(mu, par, 0) + h;
-        C2 z01 = b[0], z02 = b[(size_t)Vh], z12 = b[2 * (size_t)Vh], dg = b[3 * (size_t)Vh];
+    QCB_HD size_t index0(int mu, int par, int h) const {
+        const int nT = (int)((Vh + 31) >> 5);
+        return (size_t)((mu * 2 + par) * nT + (h >> 5)) * (4 * 32) + (h & 31);
+    }
+    __device__ __forceinline__ M3<R> load(int mu, int par, int h) const {
+        const C2* b = p + index0(mu, par, h);
+        C2 z01 = b[0], z02 = b[32], z12 = b[64], dg = b[96];
         M3<R> z;
         z(0, 1) = mkc<R>(z01.x, z01.y);
         z(0, 2) = mkc<R>(z02.x, z02.y);
@@ -146,21 +203,21 @@ struct AlgField {
         z(2, 2) = mkc<R>(0, -(dg.x + dg.y));
         return z;
     }
-    __device__ __forceinline__ void store(int mu, int par, int64_t h, const M3<R>& z) const {
-        C2* b = p + plane(mu, par, 0) + h;
+    __device__ __forceinline__ void store(int mu, int par, int h, const M3<R>& z) const {
+        C2* b = p + index0(mu, par, h);
         C2 v;
         v.x = z(0, 1).re;
         v.y = z(0, 1).im;
         b[0] = v;
         v.x = z(0, 2).re;
         v.y = z(0, 2).im;
-        b[(size_t)Vh] = v;
+        b[32] = v;
         v.x = z(1, 2).re;
         v.y = z(1, 2).im;
-        b[2 * (size_t)Vh] = v;
+        b[64] = v;
         v.x = z(0, 0).im;
         v.y = z(1, 1).im;
-        b[3 * (size_t)Vh] = v;
+        b[96] = v;
     }
 };
 

@@ -16,8 +16,10 @@ enum Fmt : int { FMT_D18 = 0, FMT_D12 = 1, FMT_F18 = 2, FMT_F12 = 3 };
 inline int fmt_of(int prec, int store) { return (prec == QCB_PREC_F32 ? 2 : 0) + (store == QCB_STORE_12 ? 1 : 0); }
 inline int fmt_ne(int fmt) { return (fmt & 1) ? 6 : 9; }
 inline size_t fmt_cbytes(int fmt) { return (fmt & 2) ? sizeof(float2) : sizeof(double2); }
-inline size_t link_bytes(int fmt, int64_t Vh) { return (size_t)8 * fmt_ne(fmt) * (size_t)Vh * fmt_cbytes(fmt); }
-inline size_t alg_bytes(int fmt, int64_t Vh) { return (size_t)8 * 4 * (size_t)Vh * fmt_cbytes(fmt); }
+// Device bytes of a link field / su(3) accumulator in the tiled layout (32-site tiles).
+inline size_t tiled_sites(int64_t Vh) { return (size_t)((Vh + 31) / 32) * 32; }
+inline size_t link_bytes(int fmt, int64_t Vh) { return (size_t)8 * fmt_ne(fmt) * tiled_sites(Vh) * fmt_cbytes(fmt); }
+inline size_t alg_bytes(int fmt, int64_t Vh) { return (size_t)8 * 4 * tiled_sites(Vh) * fmt_cbytes(fmt); }
 
 int fail(int code, const char* fmt, ...);
 // Adds n to the process-wide kernel launch counter reported by qcb_launch_count().

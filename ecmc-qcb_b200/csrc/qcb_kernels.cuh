@@ -27,18 +27,18 @@ __device__ __forceinline__ double bswap_f64(double x) {
 //   A = sum_{nu != mu} U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag + U_nu(x+mu-nu)^dag U_mu(x-nu)^dag U_nu(x-nu)
 // x has parity `par`; x+-nu and x+mu have parity 1-par; x+mu-nu has parity `par`.
 template <typename R, int NE, int MU, bool RO>
-__device__ __forceinline__ M3<R> staple(const Geom& g, const LinkField<R, NE>& U, const int c[4], int64_t lex,
+__device__ __forceinline__ M3<R> staple(const Geom& g, const LinkField<R, NE>& U, const int c[4], int lex,
                                         int par) {
     M3<R> A;
     set_zero(A);
     const int opp = par ^ 1;
-    const int64_t xmu = step_up(g, lex, c[MU], MU);
+    const int xmu = step_up(g, lex, c[MU], MU);
 #pragma unroll
     for (int nu = 0; nu < 4; nu++) {
         if (nu == MU) continue;
-        const int64_t xnu = step_up(g, lex, c[nu], nu);
-        const int64_t xmnu = step_dn(g, lex, c[nu], nu);
-        const int64_t xmumnu = step_dn(g, xmu, c[nu], nu);
+        const int xnu = step_up(g, lex, c[nu], nu);
+        const int xmnu = step_dn(g, lex, c[nu], nu);
+        const int xmumnu = step_dn(g, xmu, c[nu], nu);
         {
             M3<R> a = RO ? U.load_ro(nu, opp, xmu >> 1) : U.load(nu, opp, xmu >> 1);
             M3<R> b = RO ? U.load_ro(MU, opp, xnu >> 1) : U.load(MU, opp, xnu >> 1);
@@ -61,18 +61,18 @@ __device__ __forceinline__ M3<R> staple(const Geom& g, const LinkField<R, NE>& U
 // directions (a single kernel then serves every link class without four unrolled copies
 // competing for the instruction cache).  The nu order is the reference's (ascending, skip mu).
 template <typename R, int NE>
-__device__ __forceinline__ M3<R> staple_rt(const Geom& g, const LinkField<R, NE>& U, const int c[4], int64_t lex,
+__device__ __forceinline__ M3<R> staple_rt(const Geom& g, const LinkField<R, NE>& U, const int c[4], int lex,
                                            int par, int mu) {
     M3<R> A;
     set_zero(A);
     const int opp = par ^ 1;
-    const int64_t xmu = step_up(g, lex, c[mu], mu);
+    const int xmu = step_up(g, lex, c[mu], mu);
 #pragma unroll 1
     for (int k = 0; k < 3; k++) {
         const int nu = k < mu ? k : k + 1;
-        const int64_t xnu = step_up(g, lex, c[nu], nu);
-        const int64_t xmnu = step_dn(g, lex, c[nu], nu);
-        const int64_t xmumnu = step_dn(g, xmu, c[nu], nu);
+        const int xnu = step_up(g, lex, c[nu], nu);
+        const int xmnu = step_dn(g, lex, c[nu], nu);
+        const int xmumnu = step_dn(g, xmu, c[nu], nu);
         {
             M3<R> a = U.load_ro(nu, opp, xmu >> 1);
             M3<R> b = U.load_ro(mu, opp, xnu >> 1);
@@ -197,11 +197,11 @@ __device__ __forceinline__ void cm_subgroup(M3<R>& u, const M3<R>& A, double c_a
 // once per link, since it does not contain U(x,mu) and is therefore identical for every hit
 // (the reference recomputes it per hit).  MU >= 0 selects the direction at compile time.
 template <typename R, int NE, int MU>
-__device__ __forceinline__ void hb_link(const Geom& g, const LinkField<R, NE>& U, int par, int64_t h, double c_alpha,
+__device__ __forceinline__ void hb_link(const Geom& g, const LinkField<R, NE>& U, int par, int h, double c_alpha,
                                         int n_hits, uint64_t seed, uint32_t sweep, int reproject, int* err) {
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
-    const int64_t lex = lex_of(g, c);
+    const int lex = lex_of(g, c);
     M3<R> A = staple<R, NE, MU, true>(g, U, c, lex, par);
     M3<R> u = U.load(MU, par, h);
     LinkStream rng(seed, (uint32_t)(lex * 4 + MU), sweep, TAG_HB);
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(QCB_HB_THREADS, QCB_HB_MINB(R))
                   int reproject, int* err) {
     const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= g.Vh) return;
-    hb_link<R, NE, MU>(g, U, par, h, c_alpha, n_hits, seed, sweep, reproject, err);
+    hb_link<R, NE, MU>(g, U, par, (int)h, c_alpha, n_hits, seed, sweep, reproject, err);
 }
 
 // ------------------------------------------------------------------ Wilson flow
@@ -239,11 +239,11 @@ __global__ void __launch_bounds__(QCB_HB_THREADS, QCB_HB_MINB(R))
 // goes to a second buffer (ping-pong), which is what makes force and update one pass.
 template <typename R, int NE, int STAGE>
 __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>& Win, const LinkField<R, NE>& Wout,
-                                          const AlgField<R>& Z, double eps, int mu, int par, int64_t h,
+                                          const AlgField<R>& Z, double eps, int mu, int par, int h,
                                           int reproject) {
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
-    const int64_t lex = lex_of(g, c);
+    const int lex = lex_of(g, c);
     M3<R> A;
 #if QCB_FLOW_RTMU
     A = staple_rt<R, NE>(g, Win, c, lex, par, mu);
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(QCB_FLOW_THREADS, QCB_FLOW_MINB(R))
     const int lt = blockIdx.x & 7;
     const int64_t h = (int64_t)(blockIdx.x >> 3) * blockDim.x + threadIdx.x;
     if (h >= g.Vh) return;
-    flow_link<R, NE, STAGE>(g, Win, Wout, Z, eps, lt >> 1, lt & 1, h, reproject);
+    flow_link<R, NE, STAGE>(g, Win, Wout, Z, eps, lt >> 1, lt & 1, (int)h, reproject);
 }
 
 // ------------------------------------------------------------------ reductions
@@ -343,19 +343,19 @@ __global__ void k_finalize(const double* partials, int nb, int nv, unsigned max_
 // U_mu(x+nu)^dag U_nu(x)^dag)/3, evaluated as Re Tr((U_mu(x) U_nu(x+mu)) (U_nu(x) U_mu(x+nu))^dag).
 // Plaquette sum of one site: sum over mu<nu of Re Tr(U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag)/3
 // (observables_mpi.cpp:11-35), evaluated as Re Tr((U_mu(x) U_nu(x+mu)) (U_nu(x) U_mu(x+nu))^dag).
-template <typename R, int NE>
-__device__ __forceinline__ double site_plaquette(const Geom& g, const LinkField<R, NE>& U, int par, int64_t h) {
+template <typename R, int NE, bool TILED>
+__device__ __forceinline__ double site_plaquette(const Geom& g, const LinkField<R, NE, TILED>& U, int par, int h) {
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
-    const int64_t lex = lex_of(g, c);
+    const int lex = lex_of(g, c);
     double s = 0.0;
 #pragma unroll
     for (int mu = 0; mu < 4; mu++) {
-        const int64_t xmu = step_up(g, lex, c[mu], mu);
+        const int xmu = step_up(g, lex, c[mu], mu);
         M3<R> umu = U.load_ro(mu, par, h);
 #pragma unroll
         for (int nu = mu + 1; nu < 4; nu++) {
-            const int64_t xnu = step_up(g, lex, c[nu], nu);
+            const int xnu = step_up(g, lex, c[nu], nu);
             M3<R> p1 = mul_nn(umu, U.load_ro(nu, par ^ 1, xmu >> 1));
             M3<R> p2 = mul_nn(U.load_ro(nu, par, h), U.load_ro(mu, par ^ 1, xnu >> 1));
             s += (double)re_tr_mul_na(p1, p2) / 3.0;
@@ -364,26 +364,26 @@ __device__ __forceinline__ double site_plaquette(const Geom& g, const LinkField<
     return s;
 }
 
-template <typename R, int NE>
-__global__ void __launch_bounds__(256) k_plaquette(Geom g, LinkField<R, NE> U, double* partials) {
+template <typename R, int NE, bool TILED = true>
+__global__ void __launch_bounds__(256) k_plaquette(Geom g, LinkField<R, NE, TILED> U, double* partials) {
     const int par = blockIdx.y;
     double v[1] = {0.0};
     for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.x * blockDim.x)
-        v[0] += site_plaquette(g, U, par, h);
+        v[0] += site_plaquette(g, U, par, (int)h);
     block_sum_store<1>(v, partials, blockIdx.y * gridDim.x + blockIdx.x);
 }
 
 // clover_site (observables_mpi.cpp:66-90): F = (C - C^dag)/8 with the four leaves in the
 // reference's order and association.
 template <typename R, int NE>
-__device__ __forceinline__ M3<R> clover_F(const Geom& g, const LinkField<R, NE>& U, const int c[4], int64_t lex,
+__device__ __forceinline__ M3<R> clover_F(const Geom& g, const LinkField<R, NE>& U, const int c[4], int lex,
                                           int par, int mu, int nu) {
     const int opp = par ^ 1;
-    const int64_t xpmu = step_up(g, lex, c[mu], mu), xpnu = step_up(g, lex, c[nu], nu);
-    const int64_t xmmu = step_dn(g, lex, c[mu], mu), xmnu = step_dn(g, lex, c[nu], nu);
-    const int64_t xmmupnu = step_up(g, xmmu, c[nu], nu), xmmumnu = step_dn(g, xmmu, c[nu], nu);
-    const int64_t xpmumnu = step_dn(g, xpmu, c[nu], nu);
-    const int64_t h = lex >> 1;
+    const int xpmu = step_up(g, lex, c[mu], mu), xpnu = step_up(g, lex, c[nu], nu);
+    const int xmmu = step_dn(g, lex, c[mu], mu), xmnu = step_dn(g, lex, c[nu], nu);
+    const int xmmupnu = step_up(g, xmmu, c[nu], nu), xmmumnu = step_dn(g, xmmu, c[nu], nu);
+    const int xpmumnu = step_dn(g, xpmu, c[nu], nu);
+    const int h = lex >> 1;
     M3<R> C, t;
     // leaf 1: U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
     t = mul_nn(U.load_ro(mu, par, h), U.load_ro(nu, opp, xpmu >> 1));
@@ -413,13 +413,13 @@ __device__ __forceinline__ M3<R> clover_F(const Geom& g, const LinkField<R, NE>&
 // pair 0: +Re Tr(F01 F23), pair 1: -Re Tr(F02 F13), pair 2: +Re Tr(F03 F12); e += |F|^2/2.
 // Adds (q/(4 pi^2), e) to v.
 template <typename R, int NE>
-__device__ __forceinline__ void site_clover_pair(const Geom& g, const LinkField<R, NE>& U, int par, int pair,
-                                                 int64_t h, double v[2]) {
+__device__ __forceinline__ void site_clover_pair(const Geom& g, const LinkField<R, NE>& U, int par, int pair, int h,
+                                                 double v[2]) {
     const int a_mu = 0, a_nu = pair + 1;
     const int b_mu = (pair == 0) ? 2 : 1, b_nu = (pair == 2) ? 2 : 3;
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
-    const int64_t lex = lex_of(g, c);
+    const int lex = lex_of(g, c);
     M3<R> Fa = clover_F(g, U, c, lex, par, a_mu, a_nu);
     M3<R> Fb = clover_F(g, U, c, lex, par, b_mu, b_nu);
     double q = (double)re_tr_mul(Fa, Fb);
@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(128) k_clover_qe(Geom g, LinkField<R, NE> U, d
     const int par = blockIdx.y & 1, pair = blockIdx.y >> 1;
     double v[2] = {0.0, 0.0};
     for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.x * blockDim.x)
-        site_clover_pair(g, U, par, pair, h, v);
+        site_clover_pair(g, U, par, pair, (int)h, v);
     block_sum_store<2>(v, partials, blockIdx.y * gridDim.x + blockIdx.x);
 }
 
@@ -443,7 +443,7 @@ __global__ void __launch_bounds__(256) k_unitarity(Geom g, LinkField<R, NE> U, d
     const int mu = lt >> 1, par = lt & 1;
     double v[2] = {0.0, 0.0};
     for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.x * blockDim.x) {
-        M3<double> u = convert<double>(U.load_ro(mu, par, h));
+        M3<double> u = convert<double>(U.load_ro(mu, par, (int)h));
         M3<double> d = mul_na(u, u);
         d(0, 0).re -= 1.0;
         d(1, 1).re -= 1.0;
@@ -461,7 +461,7 @@ template <typename R, int NE>
 __global__ void k_aos_to_soa(Geom g, const double2* aos, LinkField<R, NE> U, int bswap) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= g.V * 4) return;
-    const int64_t lex = t >> 2;
+    const int lex = (int)(t >> 2);
     const int mu = (int)(t & 3);
     int c[4];
     lex_coords(g, lex, c);
@@ -482,7 +482,7 @@ template <typename R, int NE>
 __global__ void k_soa_to_aos(Geom g, LinkField<R, NE> U, double2* aos, int bswap) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= g.V * 4) return;
-    const int64_t lex = t >> 2;
+    const int lex = (int)(t >> 2);
     const int mu = (int)(t & 3);
     int c[4];
     lex_coords(g, lex, c);
@@ -516,7 +516,7 @@ __global__ void k_start(Geom g, LinkField<R, NE> U, int hot, uint64_t seed) {
     } else {
         int c[4];
         site_coords(g, par, (uint32_t)h, c);
-        const int64_t lex = lex_of(g, c);
+        const int lex = lex_of(g, c);
         LinkStream rng(seed, (uint32_t)(lex * 4 + mu), 0u, TAG_HOT);
         double gs[12];
 #pragma unroll
@@ -536,7 +536,7 @@ __global__ void k_start(Geom g, LinkField<R, NE> U, int hot, uint64_t seed) {
         }
         project_su3(m);
     }
-    U.store(mu, par, h, convert<R>(m));
+    U.store(mu, par, (int)h, convert<R>(m));
 }
 
 // U'(x) = U(x - s) (the global translation of Shift.cpp:109-160 on one periodic lattice).
@@ -556,10 +556,8 @@ __global__ void k_shift(Geom g, LinkField<R, NE> src, LinkField<R, NE> dst, int 
         c[d] = v;
     }
     const int spar = (c[0] + c[1] + c[2] + c[3]) & 1;
-    const int64_t slex = lex_of(g, c);
-    // raw element copy (no rebuild / re-encode for NE == 6)
-#pragma unroll
-    for (int e = 0; e < NE; e++) dst.p[dst.plane(mu, par, e) + h] = __ldg(src.p + src.plane(mu, spar, e) + (slex >> 1));
+    const int slex = lex_of(g, c);
+    dst.copy_from(mu, par, (int)h, src, spar, slex >> 1);
 }
 
 // projection_su3 of every link, in double (GaugeField.cpp:61-71).
@@ -569,9 +567,9 @@ __global__ void k_reunitarize(Geom g, LinkField<R, NE> U) {
     const int mu = lt >> 1, par = lt & 1;
     const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= g.Vh) return;
-    M3<double> u = convert<double>(U.load(mu, par, h));
+    M3<double> u = convert<double>(U.load(mu, par, (int)h));
     project_su3(u);
-    U.store(mu, par, h, convert<R>(u));
+    U.store(mu, par, (int)h, convert<R>(u));
 }
 
 // Staple field of one direction, written in AoS order (diagnostic entry point).
@@ -582,7 +580,7 @@ __global__ void k_staple_field(Geom g, LinkField<R, NE> U, double2* out) {
     if (h >= g.Vh) return;
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
-    const int64_t lex = lex_of(g, c);
+    const int lex = lex_of(g, c);
     M3<R> A = staple<R, NE, MU, true>(g, U, c, lex, par);
 #pragma unroll
     for (int e = 0; e < 9; e++) {

@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
         const int tile = (int)(v / TILE);
         const LatDesc* d = lattice_of(lats, tile_lat, one, tile);
         const Geom g = d->g;
-        const int64_t h = (int64_t)(tile - d->nb_begin) * TILE + (v % TILE);
+        const int h = (tile - d->nb_begin) * TILE + (int)(v % TILE);
         if (h < g.Vh)
             hb_link<R, NE, MU>(g, lview<R, NE>(d->links, g.Vh), par, h, d->c_alpha, n_hits, d->seed, sweep,
                                reproject, err);
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(QCB_FLOW_THREADS, QCB_FLOW_MINB(R))
         const Geom g = d->g;
         const int lt = t - 8 * d->nb_begin;
         const int cls = lt & 7;
-        const int64_t h = (int64_t)(lt >> 3) * TILE + threadIdx.x;
+        const int h = (lt >> 3) * TILE + threadIdx.x;
         if (h >= g.Vh) continue;
         const bool in_b = (((d->flip ^ flip_xor) + STAGE - 1) & 1) != 0;
         const LinkField<R, NE> win = lview<R, NE>(in_b ? d->links_out : d->links, g.Vh);
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(TILE)
         const Geom g = d->g;
         const int lt = t - 2 * d->nb_begin;
         const int par = lt & 1;
-        const int64_t h = (int64_t)(lt >> 1) * TILE + threadIdx.x;
+        const int h = (lt >> 1) * TILE + threadIdx.x;
         void* base = (flip_xor >= 0 && (d->flip ^ flip_xor)) ? d->links_out : d->links;
         double v[1] = {h < g.Vh ? site_plaquette(g, lview<R, NE>(base, g.Vh), par, h) : 0.0};
         block_sum_store<1>(v, partials, t);
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(TILE)
         const Geom g = d->g;
         const int lt = t - 6 * d->nb_begin;
         const int cls = lt % 6;
-        const int64_t h = (int64_t)(lt / 6) * TILE + threadIdx.x;
+        const int h = (lt / 6) * TILE + threadIdx.x;
         void* base = (flip_xor >= 0 && (d->flip ^ flip_xor)) ? d->links_out : d->links;
         double v[2] = {0.0, 0.0};
         if (h < g.Vh) site_clover_pair(g, lview<R, NE>(base, g.Vh), cls & 1, cls >> 1, h, v);
