@@ -118,79 +118,160 @@ QCB_HD int step_dn(const Geom& g, int lex, int cd, int d) {
     return (cd == 0) ? lex + (g.L[d] - 1) * g.stride[d] : lex - g.stride[d];
 }
 
+// Lexicographic offsets of the eight periodic neighbours of one site, held in registers so that
+// code with a runtime direction selects them (sel4) instead of indexing the geometry or the
+// coordinate array, which would move both into local memory.
+struct Steps {
+    int up[4], dn[4];
+};
+QCB_HD Steps make_steps(const Geom& g, const int c[4]) {
+    Steps s;
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        const int wrap = (g.L[d] - 1) * g.stride[d];
+        s.up[d] = (c[d] == g.L[d] - 1) ? -wrap : g.stride[d];
+        s.dn[d] = (c[d] == 0) ? wrap : -g.stride[d];
+    }
+    return s;
+}
+QCB_HD int sel4(const int v[4], int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : (i == 2 ? v[2] : v[3])); }
+
 // Link storage view; NE = 9 (18 reals) or 6 (12 reals, third row rebuilt on load).
+//
+// Tiled layout: the links of one (mu, parity) plane are cut into tiles of 32 consecutive
+// half-lattice sites; a tile holds NE complex elements of its 32 links, element-major, so a
+// warp reading one element of 32 neighbouring links touches one contiguous run.
+//   double: element e of lane l at tile start + e*32 + l (one 128-bit double2 per access);
+//   float:  elements (2k, 2k+1) of lane l as one float4 at tile start + k*64 + 2l, and for odd
+//           NE the last element as a float2 at tile start + (NE-1)*32 + l, so every access but
+//           that one is 128 bits wide.
+// Untiled layout (caller-owned fields): element e of link (mu, par, h) at ((mu*2+par)*NE+e)*Vh+h.
 template <typename R, int NE, bool TILED = true>
 struct LinkField {
     typedef typename V2<R>::T C2;
     C2* p;
     int64_t Vh;
-    // index of element 0 of link (mu, par, h); element e is at +e * ES
-    static constexpr int64_t kTiledStride = 32;
-    QCB_HD int64_t es() const { return TILED ? kTiledStride : Vh; }
+    static constexpr bool kQuad = TILED && sizeof(R) == 4;
+    static constexpr int kPairs = kQuad ? NE / 2 : 0;
+    // start of the tile holding link (mu, par, h)
+    QCB_HD size_t tile0(int mu, int par, int h) const {
+        const int nT = (int)((Vh + 31) >> 5);
+        return (size_t)((mu * 2 + par) * nT + (h >> 5)) * (NE * 32);
+    }
+    // element 0 of link (mu, par, h) for the 64-bit-element layouts; element e at + e * es()
+    QCB_HD int64_t es() const { return TILED ? 32 : Vh; }
     QCB_HD size_t index0(int mu, int par, int h) const {
-        if (TILED) {
-            const int nT = (int)((Vh + 31) >> 5);
-            const int tile = (mu * 2 + par) * nT + (h >> 5);
-            return (size_t)tile * (NE * 32) + (h & 31);
-        }
+        if (TILED) return tile0(mu, par, h) + (h & 31);
         return (size_t)((mu * 2 + par) * NE) * (size_t)Vh + (size_t)h;
     }
-    __device__ __forceinline__ M3<R> load(int mu, int par, int h) const {
+    template <bool RO>
+    __device__ __forceinline__ static C2 rd(const C2* a) {
+        if (RO) return __ldg(a);
+        return *a;
+    }
+    template <bool RO>
+    __device__ __forceinline__ M3<R> load_t(int mu, int par, int h) const {
         M3<R> u;
-        const C2* b = p + index0(mu, par, h);
+        if constexpr (kQuad) {
+            const C2* t = p + tile0(mu, par, h);
+            const float4* q = reinterpret_cast<const float4*>(t) + (h & 31);
 #pragma unroll
-        for (int e = 0; e < NE; e++) {
-            C2 v = b[e * es()];
-            u.e[e] = mkc<R>(v.x, v.y);
+            for (int k = 0; k < kPairs; k++) {
+                const float4 v = RO ? __ldg(q + 32 * k) : q[32 * k];
+                u.e[2 * k] = mkc<R>(v.x, v.y);
+                u.e[2 * k + 1] = mkc<R>(v.z, v.w);
+            }
+            if (NE & 1) {
+                const C2 v = rd<RO>(t + (NE - 1) * 32 + (h & 31));
+                u.e[NE - 1] = mkc<R>(v.x, v.y);
+            }
+        } else {
+            const C2* b = p + index0(mu, par, h);
+#pragma unroll
+            for (int e = 0; e < NE; e++) {
+                const C2 v = rd<RO>(b + e * es());
+                u.e[e] = mkc<R>(v.x, v.y);
+            }
         }
         if (NE == 6) rebuild_row2(u);
         return u;
     }
+    __device__ __forceinline__ M3<R> load(int mu, int par, int h) const { return load_t<false>(mu, par, h); }
     // read-only path for links that no thread of the running kernel writes
-    __device__ __forceinline__ M3<R> load_ro(int mu, int par, int h) const {
-        M3<R> u;
-        const C2* b = p + index0(mu, par, h);
-#pragma unroll
-        for (int e = 0; e < NE; e++) {
-            C2 v = __ldg(b + e * es());
-            u.e[e] = mkc<R>(v.x, v.y);
-        }
-        if (NE == 6) rebuild_row2(u);
-        return u;
-    }
+    __device__ __forceinline__ M3<R> load_ro(int mu, int par, int h) const { return load_t<true>(mu, par, h); }
     __device__ __forceinline__ void store(int mu, int par, int h, const M3<R>& u) const {
-        C2* b = p + index0(mu, par, h);
+        if constexpr (kQuad) {
+            C2* t = p + tile0(mu, par, h);
+            float4* q = reinterpret_cast<float4*>(t) + (h & 31);
 #pragma unroll
-        for (int e = 0; e < NE; e++) {
-            C2 v;
-            v.x = u.e[e].re;
-            v.y = u.e[e].im;
-            b[e * es()] = v;
+            for (int k = 0; k < kPairs; k++)
+                q[32 * k] = make_float4(u.e[2 * k].re, u.e[2 * k].im, u.e[2 * k + 1].re, u.e[2 * k + 1].im);
+            if (NE & 1) {
+                C2 v;
+                v.x = u.e[NE - 1].re;
+                v.y = u.e[NE - 1].im;
+                t[(NE - 1) * 32 + (h & 31)] = v;
+            }
+        } else {
+            C2* b = p + index0(mu, par, h);
+#pragma unroll
+            for (int e = 0; e < NE; e++) {
+                C2 v;
+                v.x = u.e[e].re;
+                v.y = u.e[e].im;
+                b[e * es()] = v;
+            }
         }
     }
     // raw element copy of one link (no rebuild / re-encode for NE == 6)
     __device__ __forceinline__ void copy_from(int mu, int par, int h, const LinkField& src, int spar, int sh) const {
-        C2* b = p + index0(mu, par, h);
-        const C2* a = src.p + src.index0(mu, spar, sh);
+        if constexpr (kQuad) {
+            C2* t = p + tile0(mu, par, h);
+            const C2* a = src.p + src.tile0(mu, spar, sh);
+            float4* q = reinterpret_cast<float4*>(t) + (h & 31);
+            const float4* r = reinterpret_cast<const float4*>(a) + (sh & 31);
 #pragma unroll
-        for (int e = 0; e < NE; e++) b[e * es()] = __ldg(a + e * src.es());
+            for (int k = 0; k < kPairs; k++) q[32 * k] = __ldg(r + 32 * k);
+            if (NE & 1) t[(NE - 1) * 32 + (h & 31)] = __ldg(a + (NE - 1) * 32 + (sh & 31));
+        } else {
+            C2* b = p + index0(mu, par, h);
+            const C2* a = src.p + src.index0(mu, spar, sh);
+#pragma unroll
+            for (int e = 0; e < NE; e++) b[e * es()] = __ldg(a + e * src.es());
+        }
     }
 };
 
-// su(3) algebra storage: 8 reals per link as 4 complex entries in the tiled layout above
+// su(3) algebra storage: 8 reals per link as 4 complex entries, tiled like LinkField
 //   0: Z01, 1: Z02, 2: Z12, 3: (Im Z00, Im Z11);  Z22 = -i(Im Z00 + Im Z11), Zji = -conj(Zij).
+// double: entry k of lane l at tile start + k*32 + l; float: entries (0,1) as one float4 at
+// tile start + 2l and entries (2,3) at tile start + 64 + 2l.
 template <typename R>
 struct AlgField {
     typedef typename V2<R>::T C2;
+    static constexpr bool kQuad = sizeof(R) == 4;
     C2* p;
     int64_t Vh;
-    QCB_HD size_t index0(int mu, int par, int h) const {
+    QCB_HD size_t tile0(int mu, int par, int h) const {
         const int nT = (int)((Vh + 31) >> 5);
-        return (size_t)((mu * 2 + par) * nT + (h >> 5)) * (4 * 32) + (h & 31);
+        return (size_t)((mu * 2 + par) * nT + (h >> 5)) * (4 * 32);
     }
     __device__ __forceinline__ M3<R> load(int mu, int par, int h) const {
-        const C2* b = p + index0(mu, par, h);
-        C2 z01 = b[0], z02 = b[32], z12 = b[64], dg = b[96];
+        C2 z01, z02, z12, dg;
+        if constexpr (kQuad) {
+            const float4* q = reinterpret_cast<const float4*>(p + tile0(mu, par, h)) + (h & 31);
+            const float4 a = q[0], b = q[32];
+            z01 = make_float2(a.x, a.y);
+            z02 = make_float2(a.z, a.w);
+            z12 = make_float2(b.x, b.y);
+            dg = make_float2(b.z, b.w);
+        } else {
+            const C2* b = p + tile0(mu, par, h) + (h & 31);
+            z01 = b[0];
+            z02 = b[32];
+            z12 = b[64];
+            dg = b[96];
+        }
         M3<R> z;
         z(0, 1) = mkc<R>(z01.x, z01.y);
         z(0, 2) = mkc<R>(z02.x, z02.y);
@@ -204,20 +285,26 @@ struct AlgField {
         return z;
     }
     __device__ __forceinline__ void store(int mu, int par, int h, const M3<R>& z) const {
-        C2* b = p + index0(mu, par, h);
-        C2 v;
-        v.x = z(0, 1).re;
-        v.y = z(0, 1).im;
-        b[0] = v;
-        v.x = z(0, 2).re;
-        v.y = z(0, 2).im;
-        b[32] = v;
-        v.x = z(1, 2).re;
-        v.y = z(1, 2).im;
-        b[64] = v;
-        v.x = z(0, 0).im;
-        v.y = z(1, 1).im;
-        b[96] = v;
+        if constexpr (kQuad) {
+            float4* q = reinterpret_cast<float4*>(p + tile0(mu, par, h)) + (h & 31);
+            q[0] = make_float4(z(0, 1).re, z(0, 1).im, z(0, 2).re, z(0, 2).im);
+            q[32] = make_float4(z(1, 2).re, z(1, 2).im, z(0, 0).im, z(1, 1).im);
+        } else {
+            C2* b = p + tile0(mu, par, h) + (h & 31);
+            C2 v;
+            v.x = z(0, 1).re;
+            v.y = z(0, 1).im;
+            b[0] = v;
+            v.x = z(0, 2).re;
+            v.y = z(0, 2).im;
+            b[32] = v;
+            v.x = z(1, 2).re;
+            v.y = z(1, 2).im;
+            b[64] = v;
+            v.x = z(0, 0).im;
+            v.y = z(1, 1).im;
+            b[96] = v;
+        }
     }
 };
 

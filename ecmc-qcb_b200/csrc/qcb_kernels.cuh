@@ -66,13 +66,15 @@ __device__ __forceinline__ M3<R> staple_rt(const Geom& g, const LinkField<R, NE>
     M3<R> A;
     set_zero(A);
     const int opp = par ^ 1;
-    const int xmu = step_up(g, lex, c[mu], mu);
+    const Steps st = make_steps(g, c);
+    const int xmu = lex + sel4(st.up, mu);
 #pragma unroll 1
     for (int k = 0; k < 3; k++) {
         const int nu = k < mu ? k : k + 1;
-        const int xnu = step_up(g, lex, c[nu], nu);
-        const int xmnu = step_dn(g, lex, c[nu], nu);
-        const int xmumnu = step_dn(g, xmu, c[nu], nu);
+        const int dnu = sel4(st.dn, nu);
+        const int xnu = lex + sel4(st.up, nu);
+        const int xmnu = lex + dnu;
+        const int xmumnu = xmu + dnu;  // x+mu has the same nu coordinate as x
         {
             M3<R> a = U.load_ro(nu, opp, xmu >> 1);
             M3<R> b = U.load_ro(mu, opp, xnu >> 1);
@@ -89,6 +91,124 @@ __device__ __forceinline__ M3<R> staple_rt(const Geom& g, const LinkField<R, NE>
         }
     }
     return A;
+}
+
+// FP32 staple with two-row products.  Every staple is a product of three SU(3) links, so it is
+// itself in SU(3) up to rounding: only its first two rows are formed by products and the third
+// is the conjugate cross product r2 = conj(r0 x r1).  Forward staple a b^dag d^dag
+// (a = U_nu(x+mu), b = U_mu(x+nu), d = U_nu(x)): rows 0-1 of a b^dag, then of (a b^dag) d^dag.
+// Backward staple t^dag v2 with t = v1 v0 (v1 = U_mu(x-nu), v0 = U_nu(x+mu-nu), v2 = U_nu(x-nu)):
+// rows 0-1 of t^dag need columns 0-1 of t only.  That is 42 instead of 54 complex
+// multiply-adds a staple.  The rebuilt row differs from the explicit product by the
+// links' distance from SU(3), which in FP32 storage is the FP32 rounding level (~1e-7).
+template <typename R, int NE>
+__device__ __forceinline__ M3<R> staple_rt_rows(const Geom& g, const LinkField<R, NE>& U, const int c[4],
+                                                int lex, int par, int mu) {
+    M3<R> A;
+    set_zero(A);
+    const int opp = par ^ 1;
+    const Steps st = make_steps(g, c);
+    const int xmu = lex + sel4(st.up, mu);
+#pragma unroll 1
+    for (int k = 0; k < 3; k++) {
+        const int nu = k < mu ? k : k + 1;
+        const int dnu = sel4(st.dn, nu);
+        const int xnu = lex + sel4(st.up, nu);
+        const int xmnu = lex + dnu;
+        const int xmumnu = xmu + dnu;  // x+mu has the same nu coordinate as x
+        {
+            const M3<R> a = U.load_ro(nu, opp, xmu >> 1);
+            const M3<R> b = U.load_ro(mu, opp, xnu >> 1);
+            Cx<R> t[2][3], s[2][3];
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    t[i][j] = mkc<R>(0, 0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) cmac_nc(t[i][j], a(i, q), b(j, q));
+                }
+            const M3<R> d = U.load_ro(nu, par, lex >> 1);
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    s[i][j] = mkc<R>(0, 0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) cmac_nc(s[i][j], t[i][q], d(j, q));
+                    A(i, j) = A(i, j) + s[i][j];
+                }
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+                cmac_cc(A(2, j), s[0][j1], s[1][j2]);
+                cmac_cc(A(2, j), mkc<R>(-s[0][j2].re, -s[0][j2].im), s[1][j1]);
+            }
+        }
+        {
+            const M3<R> v1 = U.load_ro(mu, opp, xmnu >> 1);
+            const M3<R> v0 = U.load_ro(nu, par, xmumnu >> 1);
+            Cx<R> t[3][2], s[2][3];
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    t[i][j] = mkc<R>(0, 0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) cmac(t[i][j], v1(i, q), v0(q, j));
+                }
+            const M3<R> v2 = U.load_ro(nu, opp, xmnu >> 1);
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    s[i][j] = mkc<R>(0, 0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) cmac_cn(s[i][j], t[q][i], v2(q, j));
+                    A(i, j) = A(i, j) + s[i][j];
+                }
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+                cmac_cc(A(2, j), s[0][j1], s[1][j2]);
+                cmac_cc(A(2, j), mkc<R>(-s[0][j2].re, -s[0][j2].im), s[1][j1]);
+            }
+        }
+    }
+    return A;
+}
+
+// -proj_lie(u A) (compute_force, gradient_flow.cpp:17-37) forming only the entries the
+// projection reads: the six off-diagonal entries of u A and the imaginary parts of its diagonal.
+template <typename R>
+__device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A) {
+    M3<R> m;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            if (i == j) {
+                R im = R(0);
+#pragma unroll
+                for (int q = 0; q < 3; q++) im = fma(u(i, q).re, A(q, i).im, fma(u(i, q).im, A(q, i).re, im));
+                m(i, i) = mkc<R>(R(0), im);
+            } else {
+                Cx<R> v = mkc<R>(0, 0);
+#pragma unroll
+                for (int q = 0; q < 3; q++) cmac(v, u(i, q), A(q, j));
+                m(i, j) = v;
+            }
+        }
+    M3<R> F;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            if (i != j) F(i, j) = mkc<R>(R(-0.5) * (m(i, j).re - m(j, i).re), R(-0.5) * (m(i, j).im + m(j, i).im));
+    const R tr3 = (m(0, 0).im + m(1, 1).im + m(2, 2).im) / R(3);
+#pragma unroll
+    for (int i = 0; i < 3; i++) F(i, i) = mkc<R>(R(0), tr3 - m(i, i).im);
+    return F;
 }
 
 // Launch shapes (measured on B200, 32^4): 128-thread blocks; minimum resident blocks per SM
@@ -244,21 +364,29 @@ __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>&
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
     const int lex = lex_of(g, c);
-    M3<R> A;
+    M3<R> F, u;
+    if constexpr (sizeof(R) == 4) {
+        // FP32 forms: two-row staple products and the projection's entries only
+        const M3<R> A = staple_rt_rows<R, NE>(g, Win, c, lex, par, mu);
+        u = Win.load_ro(mu, par, h);
+        F = neg_proj_lie_mul(u, A);
+    } else {
+        M3<R> A;
 #if QCB_FLOW_RTMU
-    A = staple_rt<R, NE>(g, Win, c, lex, par, mu);
+        A = staple_rt<R, NE>(g, Win, c, lex, par, mu);
 #else
-    switch (mu) {
-        case 0: A = staple<R, NE, 0, true>(g, Win, c, lex, par); break;
-        case 1: A = staple<R, NE, 1, true>(g, Win, c, lex, par); break;
-        case 2: A = staple<R, NE, 2, true>(g, Win, c, lex, par); break;
-        default: A = staple<R, NE, 3, true>(g, Win, c, lex, par); break;
-    }
+        switch (mu) {
+            case 0: A = staple<R, NE, 0, true>(g, Win, c, lex, par); break;
+            case 1: A = staple<R, NE, 1, true>(g, Win, c, lex, par); break;
+            case 2: A = staple<R, NE, 2, true>(g, Win, c, lex, par); break;
+            default: A = staple<R, NE, 3, true>(g, Win, c, lex, par); break;
+        }
 #endif
-    M3<R> u = Win.load_ro(mu, par, h);
-    M3<R> F = proj_lie(mul_nn(u, A));
+        u = Win.load_ro(mu, par, h);
+        F = proj_lie(mul_nn(u, A));
 #pragma unroll
-    for (int k = 0; k < 9; k++) F.e[k] = mkc<R>(-F.e[k].re, -F.e[k].im);  // proj_lie(-UA) = -proj_lie(UA)
+        for (int k = 0; k < 9; k++) F.e[k] = mkc<R>(-F.e[k].re, -F.e[k].im);  // proj_lie(-UA) = -proj_lie(UA)
+    }
     M3<R> X;
     if (STAGE == 1) {
         const R c1 = (R)(0.25 * eps);
@@ -376,13 +504,15 @@ __global__ void __launch_bounds__(256) k_plaquette(Geom g, LinkField<R, NE, TILE
 // clover_site (observables_mpi.cpp:66-90): F = (C - C^dag)/8 with the four leaves in the
 // reference's order and association.
 template <typename R, int NE>
-__device__ __forceinline__ M3<R> clover_F(const Geom& g, const LinkField<R, NE>& U, const int c[4], int lex,
-                                          int par, int mu, int nu) {
+__device__ __forceinline__ M3<R> clover_F(const LinkField<R, NE>& U, const Steps& st, int lex, int par, int mu,
+                                          int nu) {
     const int opp = par ^ 1;
-    const int xpmu = step_up(g, lex, c[mu], mu), xpnu = step_up(g, lex, c[nu], nu);
-    const int xmmu = step_dn(g, lex, c[mu], mu), xmnu = step_dn(g, lex, c[nu], nu);
-    const int xmmupnu = step_up(g, xmmu, c[nu], nu), xmmumnu = step_dn(g, xmmu, c[nu], nu);
-    const int xpmumnu = step_dn(g, xpmu, c[nu], nu);
+    const int upnu = sel4(st.up, nu), dnnu = sel4(st.dn, nu);
+    const int xpmu = lex + sel4(st.up, mu), xpnu = lex + upnu;
+    const int xmmu = lex + sel4(st.dn, mu), xmnu = lex + dnnu;
+    // x+-mu have the nu coordinate of x
+    const int xmmupnu = xmmu + upnu, xmmumnu = xmmu + dnnu;
+    const int xpmumnu = xpmu + dnnu;
     const int h = lex >> 1;
     M3<R> C, t;
     // leaf 1: U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
@@ -420,8 +550,9 @@ __device__ __forceinline__ void site_clover_pair(const Geom& g, const LinkField<
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
     const int lex = lex_of(g, c);
-    M3<R> Fa = clover_F(g, U, c, lex, par, a_mu, a_nu);
-    M3<R> Fb = clover_F(g, U, c, lex, par, b_mu, b_nu);
+    const Steps st = make_steps(g, c);
+    M3<R> Fa = clover_F(U, st, lex, par, a_mu, a_nu);
+    M3<R> Fb = clover_F(U, st, lex, par, b_mu, b_nu);
     double q = (double)re_tr_mul(Fa, Fb);
     v[0] += (pair == 1 ? -q : q) * (1.0 / (4.0 * kPi * kPi));
     v[1] += 0.5 * ((double)sq_norm(Fa) + (double)sq_norm(Fb));

@@ -245,6 +245,33 @@ struct ExpCoeffs {
     }
 };
 
+// Horner recurrence of exp_su3_luscher (src/su3/utils.cpp:163-186) in double for the invariants
+// t = -Re Tr(X^2)/2 and d = Re(i det X): q = (q0, q1, q2) as (re, im) pairs, with
+// exp(X) = q0 + q1 X + q2 X^2.  From q_N = c_N: q0' = c_n - i d q2, q1' = q0 - t q2, q2' = q1.
+QCB_HD void ch_coeffs(double t, double d, double q[6]) {
+    constexpr ExpCoeffs C{};
+    double q0r = C.c[18], q0i = 0.0, q1r = 0.0, q1i = 0.0, q2r = 0.0, q2i = 0.0;
+#pragma unroll
+    for (int n = 17; n >= 0; --n) {
+        double n0r = fma(d, q2i, C.c[n]);
+        double n0i = -d * q2r;
+        double n1r = fma(-t, q2r, q0r);
+        double n1i = fma(-t, q2i, q0i);
+        q2r = q1r;
+        q2i = q1i;
+        q0r = n0r;
+        q0i = n0i;
+        q1r = n1r;
+        q1i = n1i;
+    }
+    q[0] = q0r;
+    q[1] = q0i;
+    q[2] = q1r;
+    q[3] = q1i;
+    q[4] = q2r;
+    q[5] = q2i;
+}
+
 // exp_su3_luscher (src/su3/utils.cpp:145-193): exp(X), X traceless anti-Hermitian, by the
 // Cayley-Hamilton form q0 + q1 X + q2 X^2 with the N = 18 Horner recurrence.  The scalar
 // invariants and the Horner recurrence run in double for every storage precision R (the
@@ -281,23 +308,9 @@ QCB_HD M3<R> exp_su3(const M3<R>& X) {
     }
     Cx<double> dt = det3(Xd);
     double d = -dt.im;  // Re(i * det X)
-    constexpr ExpCoeffs C{};
-    double q0r = C.c[18], q0i = 0.0, q1r = 0.0, q1i = 0.0, q2r = 0.0, q2i = 0.0;
-#pragma unroll
-    for (int n = 17; n >= 0; --n) {
-        // q0' = c_n - i d q2 ; q1' = q0 - t q2 ; q2' = q1
-        double n0r = fma(d, q2i, C.c[n]);
-        double n0i = -d * q2r;
-        double n1r = fma(-t, q2r, q0r);
-        double n1i = fma(-t, q2i, q0i);
-        q2r = q1r;
-        q2i = q1i;
-        q0r = n0r;
-        q0i = n0i;
-        q1r = n1r;
-        q1i = n1i;
-    }
-    Cx<R> q0 = mkc<R>((R)q0r, (R)q0i), q1 = mkc<R>((R)q1r, (R)q1i), q2 = mkc<R>((R)q2r, (R)q2i);
+    double q[6];
+    ch_coeffs(t, d, q);
+    Cx<R> q0 = mkc<R>((R)q[0], (R)q[1]), q1 = mkc<R>((R)q[2], (R)q[3]), q2 = mkc<R>((R)q[4], (R)q[5]);
     M3<R> E;
 #pragma unroll
     for (int k = 0; k < 9; k++) {
