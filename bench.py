@@ -7,9 +7,10 @@ Workload (the "plain FP64 at scale" configuration): a 32^4 periodic SU(3) lattic
 checkerboard heatbath sweep (8 (parity, mu) passes, every link updated once with N_hits hits).
 `value` is link-updates/s over all ranks with the field resident in HBM; `e2e` is the same metric
 through the C ABI with the configuration uploaded from pinned host memory each step and the
-plaquette read back.  The flow part of the metric (site-steps/s of the Wilson flow, FP64 vs FP32
-18- and 12-real with |dQ|, dE/E and dP against FP64) is measured on the same configuration and
-reported under "flow".  Multi-GPU runs are independent replicas (weak scaling, no collective on the
+plaquette read back.  The flow part of the metric (site-steps/s of the Wilson flow over the
+configuration's 250 steps, FP64 vs FP32 18- and 12-real, the RK3 integrator alone and with clover
+Q, E and the plaquette every step, with |dQ|, dE/E and dP against FP64) is measured on the same
+configuration and reported under "flow"; each form starts from an idle GPU.  Multi-GPU runs are independent replicas (weak scaling, no collective on the
 data path).  The reference arm times the CPU restatement of the reference's heatbath on the host
 cores.
 """
@@ -227,30 +228,61 @@ def run_reference(args, rank: int, world: int):
     }), flush=True)
 
 
-def flow_block(qcb, src, prec, store, n_steps, n_warm, hbm_peak):
-    """Times n_steps RK3 steps (fused stages) and returns site-steps/s and stage-kernel roofline."""
+FLOW_STEPS = 250  # t = 5.0 at eps = 0.02: the flow of the 32^4 FP64 configuration
+FLOW_COOL_S = 2.0  # idle pause before each timed flow form
+
+
+def flow_block(qcb, src, prec, store, n_steps, hbm_peak, gpu_index=0, measured=True):
+    """One flow form on the configuration `src`, timed with CUDA events on the flow's stream.
+
+    Every form starts from the same state: an idle pause of FLOW_COOL_S first, because under the
+    1 kW power cap a form timed right after another inherits its power draw (a stage runs 10-20%
+    slower for a few hundred ms after a sustained FP64 flow).  Then
+      (a) n_steps RK3 steps after 3 warm-up steps: site-steps/s of the integrator and the mean
+          stage-kernel duration (per-launch events, for the roofline);
+      (b) if `measured`, the configuration's measured flow: the copy of `src`, n_steps RK3 steps
+          and clover Q, E and the plaquette at every one of the n_steps + 1 times
+          (qcb_flow_measure), after the same idle pause.
+    SM clocks and throttle reasons are sampled over both."""
+    V = src.V
+    time.sleep(FLOW_COOL_S)
     fl = qcb.GradientFlow(src, 0.02, prec=prec, store=store)
     f = fl.field
     stream, e0, e1 = cuda_timer(qcb, f)
-    fl.rk3_step(n_warm)
-    f.sync()
-    f.timing(True)
-    f.timing_reset()
-    e0.record(stream)
-    fl.rk3_step(n_steps)
-    e1.record(stream)
-    e1.synchronize()
-    ms = e0.elapsed_time(e1)
-    nl, kms = f.timing_read(qcb.K_FLOW)
-    f.timing(False)
-    V = src.V
+    with Clocks(gpu_index) as clk:
+        fl.rk3_step(3)
+        f.sync()
+        f.timing(True)
+        f.timing_reset()
+        e0.record(stream)
+        fl.rk3_step(n_steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        nl, kms = f.timing_read(qcb.K_FLOW)
+        f.timing(False)
+        ms_meas = None
+        if measured:
+            time.sleep(FLOW_COOL_S)
+            e0.record(stream)
+            fl.measure(src, n_steps + 1, 1, plaquette=True)
+            e1.record(stream)
+            e1.synchronize()
+            ms_meas = e0.elapsed_time(e1)
     s_u = (S_U12 if store == 1 else S_U)[prec]
     bytes_stage = V * 4 * (2 * s_u) + V * 4 * S_Z[prec] * (4 / 3)  # per stage: read+write U, Z traffic averaged
     achieved = bytes_stage / (kms / nl * 1e-3) / 1e9
     fl.close()
-    return {"site_steps_per_s": V * n_steps / (ms * 1e-3), "ms_per_rk3": ms / n_steps,
-            "stage_kernel_ms": kms / nl, "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                                                       "unit": "GB/s", "frac": achieved / hbm_peak}}
+    out = {"site_steps_per_s": V * n_steps / (ms * 1e-3), "rk3_steps": n_steps, "ms_per_rk3": ms / n_steps,
+           "stage_kernel_ms": kms / nl,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                        "frac": achieved / hbm_peak},
+           "clocks": clk.summary()}
+    if ms_meas is not None:
+        out["measured_flow"] = {"rk3_steps": n_steps, "measurements": n_steps + 1,
+                                "each": "clover Q, E and plaquette", "seconds": ms_meas * 1e-3,
+                                "site_steps_per_s": V * n_steps / (ms_meas * 1e-3)}
+    return out
 
 
 def flow_accuracy(qcb, src, n_steps):
@@ -335,6 +367,7 @@ def run_serve(qcb, n_req: int):
     steps = [int(round(x * x / 32 / 0.02)) + 1 for x in sizes]
     site_steps = sum(int(x) ** 4 * (n - 1) for x, n in zip(sizes, steps))
     srv = qcb.Server(150 << 30, prec=qcb.PREC_F32, store=qcb.STORE_18)
+    time.sleep(FLOW_COOL_S)  # both arms start from an idle GPU
     start = srv.now()
     k, done = 0, {}
     while len(done) < n_req:
@@ -352,6 +385,7 @@ def run_serve(qcb, n_req: int):
     st = srv.stats()
     srv.close()
     tq, lat2, busy = 0.0, [], 0.0
+    time.sleep(FLOW_COOL_S)
     for i in range(n_req):
         f = qcb.GaugeField((int(sizes[i]),) * 4, 64, 0)
         f.upload(inputs[i])
@@ -389,7 +423,7 @@ def run_ours(args, rank: int, world: int, local: int):
         for i in range(args.warmup):
             f.hb_sweep(BETA, N_HITS, SEED_HB, i)
         for prec, store in ((64, 0), (32, 0), (32, 1)):
-            flow_block(qcb, f, prec, store, args.steps, 2, hbm_peak)
+            flow_block(qcb, f, prec, store, args.steps, hbm_peak, local, measured=False)
         f.close()
         return
 
@@ -450,14 +484,15 @@ def run_ours(args, rank: int, world: int, local: int):
 
     # ---------------- flow: FP64 vs FP32 (18 and 12 reals) on the heatbath configuration
     flow = {}
-    n_flow = 20
-    flow["fp64"] = flow_block(qcb, f, 64, 0, n_flow, 2, hbm_peak)
-    flow["fp32_18"] = flow_block(qcb, f, 32, 0, n_flow, 2, hbm_peak)
-    flow["fp32_12"] = flow_block(qcb, f, 32, 1, n_flow, 2, hbm_peak)
+    flow["fp64"] = flow_block(qcb, f, 64, 0, FLOW_STEPS, hbm_peak, local)
+    flow["fp32_18"] = flow_block(qcb, f, 32, 0, FLOW_STEPS, hbm_peak, local)
+    flow["fp32_12"] = flow_block(qcb, f, 32, 1, FLOW_STEPS, hbm_peak, local)
     acc = flow_accuracy(qcb, f, 40)
     for k in ("fp32_18", "fp32_12"):
         flow[k].update(acc[k])
         flow[k]["speedup_vs_fp64"] = flow[k]["site_steps_per_s"] / flow["fp64"]["site_steps_per_s"]
+        flow[k]["measured_flow"]["speedup_vs_fp64"] = (flow[k]["measured_flow"]["site_steps_per_s"] /
+                                                       flow["fp64"]["measured_flow"]["site_steps_per_s"])
 
     # ---------------- heatbath variants on the same lattice: N_hits = 1, FP32 links
     hb_more = {}

@@ -211,8 +211,10 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
     return F;
 }
 
-// Launch shapes (measured on B200, 32^4): 128-thread blocks; minimum resident blocks per SM
-// 3 for FP64 (<= 168 registers, no spills) and 4 for FP32 (<= 128 registers, no spills).
+// Launch shapes (measured on B200, 32^4): 128-thread blocks.  Minimum resident blocks per SM:
+// heatbath 3 for FP64 (<= 168 registers; 4 is slower) and 4 for FP32 (<= 128); flow stages 3
+// for FP64 (<= 168 registers; 4 is no faster) and 6 for FP32 (<= 80 registers, no spills:
+// 0.36 ms a stage against 0.40 ms at 4 and 0.37 ms at 8).
 #ifndef QCB_HB_THREADS
 #define QCB_HB_THREADS 128
 #endif
@@ -223,7 +225,7 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
 #define QCB_FLOW_THREADS 128
 #endif
 #ifndef QCB_FLOW_MINB
-#define QCB_FLOW_MINB(R) (sizeof(R) == 8 ? 3 : 4)
+#define QCB_FLOW_MINB(R) (sizeof(R) == 8 ? 3 : 6)
 #endif
 #ifndef QCB_FLOW_RTMU
 #define QCB_FLOW_RTMU 1
@@ -330,11 +332,7 @@ __device__ __forceinline__ void hb_link(const Geom& g, const LinkField<R, NE>& U
         cm_subgroup<R, 1, 2>(u, A, c_alpha, rng, err);
         cm_subgroup<R, 0, 2>(u, A, c_alpha, rng, err);
     }
-    if (reproject) {
-        M3<double> ud = convert<double>(u);
-        project_su3(ud);
-        u = convert<R>(ud);
-    }
+    if (reproject) reproject_fp64(u);
     U.store(MU, par, h, u);
 }
 
@@ -412,11 +410,7 @@ __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>&
     }
     M3<R> E = exp_su3(X);
     M3<R> w = mul_nn(E, u);
-    if (reproject) {
-        M3<double> wd = convert<double>(w);
-        project_su3(wd);
-        w = convert<R>(wd);
-    }
+    if (reproject) reproject_fp64(w);
     Wout.store(mu, par, h, w);
 }
 

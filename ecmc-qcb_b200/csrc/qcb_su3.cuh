@@ -272,6 +272,25 @@ QCB_HD void ch_coeffs(double t, double d, double q[6]) {
     q[5] = q2i;
 }
 
+// Invariants t = -Re Tr(X^2)/2 and d = Re(i det X) of an anti-Hermitian X (X_ji = -conj(X_ij),
+// zero real diagonal) in double from its independent entries.  With X = iH and a_i = Im X_ii:
+//   t = |X01|^2 + |X02|^2 + |X12|^2 + (a0^2 + a1^2 + a2^2)/2,
+//   d = det H = a0 a1 a2 + 2 Im(X01 X12 conj(X02)) - a0 |X12|^2 - a1 |X02|^2 - a2 |X01|^2.
+// Nine conversions to double instead of eighteen; used for FP32 X, whose force and RK3 forms
+// keep the anti-Hermitian symmetry exactly.
+template <typename R>
+QCB_HD void su3_invariants(const M3<R>& X, double& t, double& d) {
+    const double x01r = X(0, 1).re, x01i = X(0, 1).im, x02r = X(0, 2).re, x02i = X(0, 2).im;
+    const double x12r = X(1, 2).re, x12i = X(1, 2).im;
+    const double a0 = X(0, 0).im, a1 = X(1, 1).im, a2 = X(2, 2).im;
+    const double n01 = fma(x01r, x01r, x01i * x01i), n02 = fma(x02r, x02r, x02i * x02i);
+    const double n12 = fma(x12r, x12r, x12i * x12i);
+    t = (n01 + n02) + n12 + 0.5 * (fma(a0, a0, fma(a1, a1, a2 * a2)));
+    const double pr = fma(x01r, x12r, -x01i * x12i), pi = fma(x01r, x12i, x01i * x12r);  // X01 X12
+    const double im3 = fma(pi, x02r, -pr * x02i);                                         // Im(p conj(X02))
+    d = fma(a0 * a1, a2, fma(2.0, im3, -fma(a0, n12, fma(a1, n02, a2 * n01))));
+}
+
 // exp_su3_luscher (src/su3/utils.cpp:145-193): exp(X), X traceless anti-Hermitian, by the
 // Cayley-Hamilton form q0 + q1 X + q2 X^2 with the N = 18 Horner recurrence.  The scalar
 // invariants and the Horner recurrence run in double for every storage precision R (the
@@ -293,21 +312,14 @@ QCB_HD M3<R> exp_su3(const M3<R>& X) {
     X2(2, 0) = cconj(X2(0, 2));
     X2(2, 1) = cconj(X2(1, 2));
     X2(0, 0).im = X2(1, 1).im = X2(2, 2).im = R(0);
-    M3<double> Xd = convert<double>(X);
-    double t;
-    if (sizeof(R) == sizeof(double)) {
+    double t, d;
+    if constexpr (sizeof(R) == sizeof(double)) {
+        const M3<double> Xd = convert<double>(X);
         t = -0.5 * (((double)X2(0, 0).re + (double)X2(1, 1).re) + (double)X2(2, 2).re);
+        d = -det3(Xd).im;  // Re(i * det X)
     } else {
-        // Re Tr(X^2) in double from the same entries
-        double s = 0.0;
-#pragma unroll
-        for (int i = 0; i < 3; i++)
-#pragma unroll
-            for (int k = 0; k < 3; k++) s = fma(Xd(i, k).re, Xd(k, i).re, fma(-Xd(i, k).im, Xd(k, i).im, s));
-        t = -0.5 * s;
+        su3_invariants(X, t, d);
     }
-    Cx<double> dt = det3(Xd);
-    double d = -dt.im;  // Re(i * det X)
     double q[6];
     ch_coeffs(t, d, q);
     Cx<R> q0 = mkc<R>((R)q[0], (R)q[1]), q1 = mkc<R>((R)q[2], (R)q[3]), q2 = mkc<R>((R)q[4], (R)q[5]);
@@ -356,6 +368,75 @@ QCB_HD void project_su3(M3<R>& U) {
     U(0, 2) = cconj(c0[1] * c1[2] - c0[2] * c1[1]);
     U(1, 2) = cconj(c0[2] * c1[0] - c0[0] * c1[2]);
     U(2, 2) = cconj(c0[0] * c1[1] - c0[1] * c1[0]);
+}
+
+// projection_su3 (src/gauge/GaugeField.cpp:36-58) of an FP32 matrix with the Gram-Schmidt
+// arithmetic in double: the first two columns are widened (the third is discarded by the
+// projection), each inverse norm is one Newton step y (3 - n y^2) / 2 in double from the FP32
+// rsqrtf estimate (relative error ~1e-13, five orders below FP32 rounding), and the result is
+// rounded to FP32 once.
+QCB_HD void project_su3_f32(M3<float>& U) {
+    double c0r[3], c0i[3], c1r[3], c1i[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        c0r[i] = U(i, 0).re;
+        c0i[i] = U(i, 0).im;
+        c1r[i] = U(i, 1).re;
+        c1i[i] = U(i, 1).im;
+    }
+    auto inv_sqrt = [](double n) {
+#ifdef __CUDA_ARCH__
+        const double y = (double)rsqrtf((float)n);
+#else
+        const double y = (double)(1.0f / sqrtf((float)n));
+#endif
+        return y * fma(-0.5 * n, y * y, 1.5);
+    };
+    const double n0 = fma(c0r[0], c0r[0], c0i[0] * c0i[0]) + fma(c0r[1], c0r[1], c0i[1] * c0i[1]) +
+                      fma(c0r[2], c0r[2], c0i[2] * c0i[2]);
+    const double y0 = inv_sqrt(n0);
+    double dr = 0.0, di = 0.0;  // conj(c0) . c1
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        c0r[i] *= y0;
+        c0i[i] *= y0;
+        dr = fma(c0r[i], c1r[i], fma(c0i[i], c1i[i], dr));
+        di = fma(c0r[i], c1i[i], fma(-c0i[i], c1r[i], di));
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        c1r[i] -= fma(c0r[i], dr, -c0i[i] * di);
+        c1i[i] -= fma(c0r[i], di, c0i[i] * dr);
+    }
+    const double n1 = fma(c1r[0], c1r[0], c1i[0] * c1i[0]) + fma(c1r[1], c1r[1], c1i[1] * c1i[1]) +
+                      fma(c1r[2], c1r[2], c1i[2] * c1i[2]);
+    const double y1 = inv_sqrt(n1);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        c1r[i] *= y1;
+        c1i[i] *= y1;
+        U(i, 0) = mkc<float>((float)c0r[i], (float)c0i[i]);
+        U(i, 1) = mkc<float>((float)c1r[i], (float)c1i[i]);
+    }
+    // c2 = conj(c0 x c1)
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const int a = (i + 1) % 3, b = (i + 2) % 3;
+        const double re = fma(c0r[a], c1r[b], -c0i[a] * c1i[b]) - fma(c0r[b], c1r[a], -c0i[b] * c1i[a]);
+        const double im = fma(c0r[a], c1i[b], c0i[a] * c1r[b]) - fma(c0r[b], c1i[a], c0i[b] * c1r[a]);
+        U(i, 2) = mkc<float>((float)re, (float)-im);
+    }
+}
+
+// SU(3) reprojection in double after an FP64 or FP32 update: projection_su3 on double links,
+// project_su3_f32 on FP32 links.
+template <typename R>
+QCB_HD void reproject_fp64(M3<R>& U) {
+    if constexpr (sizeof(R) == sizeof(double)) {
+        project_su3(U);
+    } else {
+        project_su3_f32(U);
+    }
 }
 
 // Third row of an SU(3) matrix from its first two: r2 = conj(r0 x r1).
