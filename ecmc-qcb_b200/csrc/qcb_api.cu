@@ -145,11 +145,12 @@ int enq_plaquette(qcb_field_s* f, double* dst) {
     RET(launch(f, QCB_K_PLAQ, [&] { return fmt_ops(f->fmt).plaquette(f->g, f->links, f->partials, nbx, f->stream); }));
     return finalize(f, (int)(nbx * 2), 1, 0u, dst);
 }
+// Clover sums (q, e, plaquette) -> dst[0..2]; the plaquette sum comes from leaf 1 of each plane.
 int enq_clover(qcb_field_s* f, double* dst) {
     const unsigned nbx = red_blocks(f->g.Vh, 128);
-    RET(ensure_partials(f, (size_t)nbx * 6 * 2));
+    RET(ensure_partials(f, (size_t)nbx * 6 * 3));
     RET(launch(f, QCB_K_CLOVER, [&] { return fmt_ops(f->fmt).clover(f->g, f->links, f->partials, nbx, f->stream); }));
-    return finalize(f, (int)(nbx * 6), 2, 0u, dst);
+    return finalize(f, (int)(nbx * 6), 3, 0u, dst);
 }
 
 int read_results(qcb_field_s* f, int n) {
@@ -587,8 +588,7 @@ int qcb_flow_measure(qcb_flow fl, qcb_field src, int n_steps, int n_rk, double* 
     CK(cudaMallocAsync((void**)&d_meas, (size_t)n_steps * 3 * sizeof(double), f->stream));
     int r = QCB_OK;
     for (int s = 0; s < n_steps && r == QCB_OK; s++) {
-        r = enq_clover(f, d_meas + 3 * s);
-        if (r == QCB_OK && plaq) r = enq_plaquette(f, d_meas + 3 * s + 2);
+        r = enq_clover(f, d_meas + 3 * s);  // q, e and the plaquette sum
         if (r == QCB_OK && s != n_steps - 1) r = qcb_flow_rk3(fl, n_rk);
     }
     std::vector<double> h((size_t)n_steps * 3);

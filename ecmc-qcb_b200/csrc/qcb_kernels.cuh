@@ -227,6 +227,11 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
 #ifndef QCB_FLOW_MINB
 #define QCB_FLOW_MINB(R) (sizeof(R) == 8 ? 3 : 6)
 #endif
+// Clover kernels: 2 resident blocks per SM for FP64, 4 for FP32 (32^4 clover pass 1.02 ms FP64 and
+// 0.49 ms FP32 against 1.24 ms and 0.69 ms at 3 and 6).
+#ifndef QCB_CLOVER_MINB
+#define QCB_CLOVER_MINB(R) (sizeof(R) == 8 ? 2 : 4)
+#endif
 #ifndef QCB_FLOW_RTMU
 #define QCB_FLOW_RTMU 1
 #endif
@@ -495,11 +500,94 @@ __global__ void __launch_bounds__(256) k_plaquette(Geom g, LinkField<R, NE, TILE
     block_sum_store<1>(v, partials, blockIdx.y * gridDim.x + blockIdx.x);
 }
 
-// clover_site (observables_mpi.cpp:66-90): F = (C - C^dag)/8 with the four leaves in the
-// reference's order and association.
+// Clover field strength F = (C - C^dag)/8 (clover_site, observables_mpi.cpp:66-90) held as its
+// nine independent reals: F is exactly anti-Hermitian, so only the upper off-diagonal entries
+// o = (F01, F02, F12) and the imaginary diagonal d_i = Im F_ii are kept.
+template <typename R>
+struct CloverF {
+    Cx<R> o[3];
+    R d[3];
+};
+
+// Adds leaf L to the clover sums: o_ij += L_ij - conj(L_ji) (i < j), d_i += Im L_ii.
+template <typename R>
+__device__ __forceinline__ void clover_acc(CloverF<R>& S, const M3<R>& L) {
+    S.o[0] = S.o[0] + (L(0, 1) - cconj(L(1, 0)));
+    S.o[1] = S.o[1] + (L(0, 2) - cconj(L(2, 0)));
+    S.o[2] = S.o[2] + (L(1, 2) - cconj(L(2, 1)));
+#pragma unroll
+    for (int i = 0; i < 3; i++) S.d[i] += L(i, i).im;
+}
+
+// Row i of a link or of its adjoint.
+template <typename R, bool DAG>
+__device__ __forceinline__ void link_row(const M3<R>& A, int i, Cx<R> r[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) r[k] = DAG ? cconj(A(k, i)) : A(i, k);
+}
+// r <- r B (DAG = false) or r B^dag (DAG = true) for the two rows r[0], r[1].
+template <typename R, bool DAG>
+__device__ __forceinline__ void rows_mul(Cx<R> r[2][3], const M3<R>& B) {
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        Cx<R> n[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            n[j] = mkc<R>(0, 0);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                if (DAG)
+                    cmac_nc(n[j], r[i][k], B(j, k));
+                else
+                    cmac(n[j], r[i][k], B(k, j));
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 3; j++) r[i][j] = n[j];
+    }
+}
+// Full SU(3) matrix from its first two rows: r2 = conj(r0 x r1).
+template <typename R>
+__device__ __forceinline__ M3<R> from_rows(const Cx<R> r[2][3]) {
+    M3<R> L;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        L(0, j) = r[0][j];
+        L(1, j) = r[1][j];
+        const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+        L(2, j) = cconj(r[0][j1] * r[1][j2] - r[0][j2] * r[1][j1]);
+    }
+    return L;
+}
+
+// One clover leaf A' B' C' D' (' = adjoint where the flag is set).  FP64 multiplies full
+// matrices in the reference's association ((A' B') C') D'; FP32 carries the first two rows
+// through the three products and rebuilds the third row of the SU(3) leaf (60 instead of 81
+// complex multiply-adds; the rebuilt row differs from the product by the links' distance from
+// SU(3), the FP32 rounding level).
+template <typename R, bool DA, bool DB, bool DC, bool DD>
+__device__ __forceinline__ M3<R> clover_leaf(const M3<R>& A, const M3<R>& B, const M3<R>& C, const M3<R>& D) {
+    if constexpr (sizeof(R) == 4) {
+        Cx<R> r[2][3];
+        link_row<R, DA>(A, 0, r[0]);
+        link_row<R, DA>(A, 1, r[1]);
+        rows_mul<R, DB>(r, B);
+        rows_mul<R, DC>(r, C);
+        rows_mul<R, DD>(r, D);
+        return from_rows(r);
+    } else {
+        const M3<R> a = DA ? adjoint(A) : A;
+        M3<R> t = DB ? mul_na(a, B) : mul_nn(a, B);
+        t = DC ? mul_na(t, C) : mul_nn(t, C);
+        return DD ? mul_na(t, D) : mul_nn(t, D);
+    }
+}
+
+// F of plane (mu, nu) at site x with the four leaves in the reference's order; also returns
+// Re Tr of leaf 1, which is the plaquette U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag.
 template <typename R, int NE>
-__device__ __forceinline__ M3<R> clover_F(const LinkField<R, NE>& U, const Steps& st, int lex, int par, int mu,
-                                          int nu) {
+__device__ __forceinline__ CloverF<R> clover_F(const LinkField<R, NE>& U, const Steps& st, int lex, int par, int mu,
+                                               int nu, R& plaq_tr) {
     const int opp = par ^ 1;
     const int upnu = sel4(st.up, nu), dnnu = sel4(st.dn, nu);
     const int xpmu = lex + sel4(st.up, mu), xpnu = lex + upnu;
@@ -508,57 +596,92 @@ __device__ __forceinline__ M3<R> clover_F(const LinkField<R, NE>& U, const Steps
     const int xmmupnu = xmmu + upnu, xmmumnu = xmmu + dnnu;
     const int xpmumnu = xpmu + dnnu;
     const int h = lex >> 1;
-    M3<R> C, t;
+    CloverF<R> S;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        S.o[k] = mkc<R>(0, 0);
+        S.d[k] = R(0);
+    }
+    M3<R> L;
     // leaf 1: U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
-    t = mul_nn(U.load_ro(mu, par, h), U.load_ro(nu, opp, xpmu >> 1));
-    t = mul_na(t, U.load_ro(mu, opp, xpnu >> 1));
-    C = mul_na(t, U.load_ro(nu, par, h));
+    L = clover_leaf<R, false, false, true, true>(U.load_ro(mu, par, h), U.load_ro(nu, opp, xpmu >> 1),
+                                                 U.load_ro(mu, opp, xpnu >> 1), U.load_ro(nu, par, h));
+    plaq_tr = (L(0, 0).re + L(1, 1).re) + L(2, 2).re;
+    clover_acc(S, L);
     // leaf 2: U_nu(x) U_mu(x-mu+nu)^dag U_nu(x-mu)^dag U_mu(x-mu)
-    t = mul_na(U.load_ro(nu, par, h), U.load_ro(mu, par, xmmupnu >> 1));
-    t = mul_na(t, U.load_ro(nu, opp, xmmu >> 1));
-    acc_nn(C, t, U.load_ro(mu, opp, xmmu >> 1));
+    L = clover_leaf<R, false, true, true, false>(U.load_ro(nu, par, h), U.load_ro(mu, par, xmmupnu >> 1),
+                                                 U.load_ro(nu, opp, xmmu >> 1), U.load_ro(mu, opp, xmmu >> 1));
+    clover_acc(S, L);
     // leaf 3: U_mu(x-mu)^dag U_nu(x-mu-nu)^dag U_mu(x-mu-nu) U_nu(x-nu)
-    t = mul_nn(U.load_ro(nu, par, xmmumnu >> 1), U.load_ro(mu, opp, xmmu >> 1));
-    t = mul_an(t, U.load_ro(mu, par, xmmumnu >> 1));
-    acc_nn(C, t, U.load_ro(nu, opp, xmnu >> 1));
+    L = clover_leaf<R, true, true, false, false>(U.load_ro(mu, opp, xmmu >> 1), U.load_ro(nu, par, xmmumnu >> 1),
+                                                 U.load_ro(mu, par, xmmumnu >> 1), U.load_ro(nu, opp, xmnu >> 1));
+    clover_acc(S, L);
     // leaf 4: U_nu(x-nu)^dag U_mu(x-nu) U_nu(x+mu-nu) U_mu(x)^dag
-    t = mul_an(U.load_ro(nu, opp, xmnu >> 1), U.load_ro(mu, opp, xmnu >> 1));
-    t = mul_nn(t, U.load_ro(nu, par, xpmumnu >> 1));
-    acc_na(C, t, U.load_ro(mu, par, h));
-    M3<R> F;
+    L = clover_leaf<R, true, false, false, true>(U.load_ro(nu, opp, xmnu >> 1), U.load_ro(mu, opp, xmnu >> 1),
+                                                 U.load_ro(nu, par, xpmumnu >> 1), U.load_ro(mu, par, h));
+    clover_acc(S, L);
 #pragma unroll
-    for (int i = 0; i < 3; i++)
+    for (int k = 0; k < 3; k++) {
+        S.o[k] = scl((R)0.125, S.o[k]);
+        S.d[k] = (R)0.25 * S.d[k];  // Im F_ii = (Im C_ii - (-Im C_ii)) / 8
+    }
+    return S;
+}
+
+// Re Tr(Fa Fb) and |F|^2 of anti-Hermitian matrices from their nine reals:
+//   Re Tr(Fa Fb) = -2 sum_k Re(oa_k conj(ob_k)) - sum_i da_i db_i,  |F|^2 = 2 sum_k |o_k|^2 + sum_i d_i^2.
+template <typename R>
+__device__ __forceinline__ double clover_re_tr(const CloverF<R>& a, const CloverF<R>& b) {
+    double s = 0.0, t = 0.0;
 #pragma unroll
-        for (int j = 0; j < 3; j++) F(i, j) = scl((R)0.125, C(i, j) - cconj(C(j, i)));
-    return F;
+    for (int k = 0; k < 3; k++) {
+        s += (double)a.o[k].re * (double)b.o[k].re + (double)a.o[k].im * (double)b.o[k].im;
+        t += (double)a.d[k] * (double)b.d[k];
+    }
+    return -2.0 * s - t;
+}
+template <typename R>
+__device__ __forceinline__ double clover_sq_norm(const CloverF<R>& a) {
+    double s = 0.0, t = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        s += (double)a.o[k].re * (double)a.o[k].re + (double)a.o[k].im * (double)a.o[k].im;
+        t += (double)a.d[k] * (double)a.d[k];
+    }
+    return 2.0 * s + t;
 }
 
 // local_q_e_clover (observables_mpi.cpp:93-112) for one (site, plane pair):
 // pair 0: +Re Tr(F01 F23), pair 1: -Re Tr(F02 F13), pair 2: +Re Tr(F03 F12); e += |F|^2/2.
-// Adds (q/(4 pi^2), e) to v.
-template <typename R, int NE>
+// Adds (q/(4 pi^2), e) to v[0], v[1] and, with NV = 3, the plaquette sum Re Tr(leaf 1)/3 of the
+// pair's two planes to v[2] (the three pairs cover the six planes once).
+template <typename R, int NE, int NV>
 __device__ __forceinline__ void site_clover_pair(const Geom& g, const LinkField<R, NE>& U, int par, int pair, int h,
-                                                 double v[2]) {
+                                                 double v[NV]) {
     const int a_mu = 0, a_nu = pair + 1;
     const int b_mu = (pair == 0) ? 2 : 1, b_nu = (pair == 2) ? 2 : 3;
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
     const int lex = lex_of(g, c);
     const Steps st = make_steps(g, c);
-    M3<R> Fa = clover_F(U, st, lex, par, a_mu, a_nu);
-    M3<R> Fb = clover_F(U, st, lex, par, b_mu, b_nu);
-    double q = (double)re_tr_mul(Fa, Fb);
+    R pa, pb;
+    const CloverF<R> Fa = clover_F(U, st, lex, par, a_mu, a_nu, pa);
+    const CloverF<R> Fb = clover_F(U, st, lex, par, b_mu, b_nu, pb);
+    const double q = clover_re_tr(Fa, Fb);
     v[0] += (pair == 1 ? -q : q) * (1.0 / (4.0 * kPi * kPi));
-    v[1] += 0.5 * ((double)sq_norm(Fa) + (double)sq_norm(Fb));
+    v[1] += 0.5 * (clover_sq_norm(Fa) + clover_sq_norm(Fb));
+    if constexpr (NV == 3) v[2] += ((double)pa + (double)pb) / 3.0;
 }
 
+// Clover Q/E of one field: grid (site blocks, 6 = parity x plane pair); partials (q, e, p) per
+// block, p the plaquette sum of the block's planes.
 template <typename R, int NE>
-__global__ void __launch_bounds__(128) k_clover_qe(Geom g, LinkField<R, NE> U, double* partials) {
+__global__ void __launch_bounds__(128, QCB_CLOVER_MINB(R)) k_clover_qe(Geom g, LinkField<R, NE> U, double* partials) {
     const int par = blockIdx.y & 1, pair = blockIdx.y >> 1;
-    double v[2] = {0.0, 0.0};
+    double v[3] = {0.0, 0.0, 0.0};
     for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.x * blockDim.x)
-        site_clover_pair(g, U, par, pair, (int)h, v);
-    block_sum_store<2>(v, partials, blockIdx.y * gridDim.x + blockIdx.x);
+        site_clover_pair<R, NE, 3>(g, U, par, pair, (int)h, v);
+    block_sum_store<3>(v, partials, blockIdx.y * gridDim.x + blockIdx.x);
 }
 
 // Unitarity error ||U U^dag - 1||_F per link (src/bin/test.cpp:58-72): partials (max, sum).

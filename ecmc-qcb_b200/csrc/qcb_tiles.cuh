@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(TILE)
 
 // Clover Q/E: 6 tiles per block (parity x plane pair); two partials (q, e) per tile.
 template <typename R, int NE>
-__global__ void __launch_bounds__(TILE)
+__global__ void __launch_bounds__(TILE, QCB_CLOVER_MINB(R))
     k_clover_tiles(const LatDesc* __restrict__ lats, const int* __restrict__ tile_lat, const LatDesc one, int ntiles,
                    int flip_xor, double* partials) {
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(TILE)
         const int h = (lt / 6) * TILE + threadIdx.x;
         void* base = (flip_xor >= 0 && (d->flip ^ flip_xor)) ? d->links_out : d->links;
         double v[2] = {0.0, 0.0};
-        if (h < g.Vh) site_clover_pair(g, lview<R, NE>(base, g.Vh), cls & 1, cls >> 1, h, v);
+        if (h < g.Vh) site_clover_pair<R, NE, 2>(g, lview<R, NE>(base, g.Vh), cls & 1, cls >> 1, h, v);
         block_sum_store<2>(v, partials, t);
         __syncthreads();
     }
