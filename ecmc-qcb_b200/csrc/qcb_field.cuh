@@ -9,10 +9,10 @@
 // HBM layout of one field ("parity-split, tiled structure of arrays"):
 //     plane(mu, parity) = mu*2 + parity, tile = h / 32, lane = h % 32  (h = lex/2)
 //     element e of link (mu, parity, h) = base[((plane * nT + tile) * NE + e) * 32 + lane]
-// with one complex per element and nT = ceil(V/2 / 32).  Lx is even, so the two sites 2k, 2k+1
-// of an x-row have opposite parity and share h = k.  A warp of 32 consecutive h reads 32
-// consecutive complexes for every element (fully coalesced 16-byte FP64 / 8-byte FP32 accesses),
-// and the NE elements of one link sit at compile-time offsets e*32 from one base address, so a
+// with one complex per element and nT = ceil(V/2 / 32) (FP32 tiles pair the elements into 128-bit
+// words, see LinkField).  Lx is even, so the two sites 2k, 2k+1 of an x-row have opposite parity
+// and share h = k.  A warp of 32 consecutive h reads one contiguous run per element (or element
+// pair), and the elements of one link sit at compile-time offsets from one base address, so a
 // link load costs one address computation.  NE = 9 stores the full matrix (18 reals); NE = 6 the
 // first two rows (12 reals), the third rebuilt in registers as conj(row0 x row1).
 // The untiled variant (TILED = false: element e at base[(plane*NE + e)*V/2 + h]) is the layout of
@@ -318,14 +318,10 @@ QCB_HD void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
             k0 += W0;
             k1 += W1;
         }
-#ifdef __CUDA_ARCH__
-        uint32_t hi0 = __umulhi(M0, c[0]), lo0 = M0 * c[0];
-        uint32_t hi1 = __umulhi(M1, c[2]), lo1 = M1 * c[2];
-#else
-        uint64_t p0 = (uint64_t)M0 * c[0], p1 = (uint64_t)M1 * c[2];
-        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
-        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
-#endif
+        // one 32x32 -> 64-bit product gives both halves
+        const uint64_t p0 = (uint64_t)M0 * c[0], p1 = (uint64_t)M1 * c[2];
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
         uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
         c[0] = n0;
         c[1] = lo1;
@@ -351,6 +347,16 @@ struct LinkStream {
     QCB_HD LinkStream(uint64_t seed, uint32_t link_, uint32_t sweep_, uint32_t tag_)
         : k0((uint32_t)seed), k1((uint32_t)(seed >> 32)), link(link_), sweep(sweep_), tag(tag_), n(0), spare(0),
           has(false) {}
+    // The two doubles of Philox call n, (u53(w0, w1), u53(w2, w3)): draws 2n and 2n+1 of the
+    // stream, without touching the stream's position.
+    QCB_HD double2 call(uint32_t n_) const {
+        uint32_t c[4] = {n_, link, sweep, tag};
+        philox4x32_10(c, k0, k1);
+        double2 r;
+        r.x = u53(c[0], c[1]);
+        r.y = u53(c[2], c[3]);
+        return r;
+    }
     QCB_HD double next() {
         if (has) {
             has = false;

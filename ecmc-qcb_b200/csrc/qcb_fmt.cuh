@@ -43,9 +43,9 @@ struct FmtImpl {
                              int rep, int* err, cudaStream_t s) {
         constexpr bool f64 = sizeof(R) == 8;
         switch (variant) {
-            case 0: return hb_launch<MU, 64, f64 ? 6 : 8>(w, par, n_hits, sd, sa, rep, err, s);
+            case 0: return hb_launch<MU, 64, f64 ? 8 : 12>(w, par, n_hits, sd, sa, rep, err, s);
             case 2: return hb_launch<MU, 256, 2>(w, par, n_hits, sd, sa, rep, err, s);
-            default: return hb_launch<MU, 128, f64 ? 3 : 4>(w, par, n_hits, sd, sa, rep, err, s);
+            default: return hb_launch<MU, 128, f64 ? 4 : 6>(w, par, n_hits, sd, sa, rep, err, s);
         }
     }
     static cudaError_t hb(const WorkList& w, int variant, int par, int mu, int n_hits, const uint32_t* sd, uint32_t sa,
@@ -181,8 +181,8 @@ struct FmtImpl {
         o.reunitarize = &reunitarize;
         o.staple_field = &staple_field;
         constexpr bool f64 = sizeof(R) == 8;
-        o.hb_variant_name[0] = f64 ? "64x6" : "64x8";
-        o.hb_variant_name[1] = f64 ? "128x3" : "128x4";
+        o.hb_variant_name[0] = f64 ? "64x8" : "64x12";
+        o.hb_variant_name[1] = f64 ? "128x4" : "128x6";
         o.hb_variant_name[2] = "256x2";
         return o;
     }

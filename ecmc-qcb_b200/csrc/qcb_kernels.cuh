@@ -212,14 +212,14 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
 }
 
 // Launch shapes (measured on B200, 32^4): 128-thread blocks.  Minimum resident blocks per SM:
-// heatbath 3 for FP64 (<= 168 registers; 4 is slower) and 4 for FP32 (<= 128); flow stages 3
-// for FP64 (<= 168 registers; 4 is no faster) and 6 for FP32 (<= 80 registers, no spills:
-// 0.36 ms a stage against 0.40 ms at 4 and 0.37 ms at 8).
+// heatbath 4 for FP64 (<= 128 registers; 0.236 ms a sub-sweep at N_hits = 2 against 0.245 ms at
+// 3) and 6 for FP32; flow stages 3 for FP64 (<= 168 registers; 4 is no faster) and 6 for FP32
+// (<= 80 registers, no spills: 0.36 ms a stage against 0.40 ms at 4 and 0.37 ms at 8).
 #ifndef QCB_HB_THREADS
 #define QCB_HB_THREADS 128
 #endif
 #ifndef QCB_HB_MINB
-#define QCB_HB_MINB(R) (sizeof(R) == 8 ? 3 : 4)
+#define QCB_HB_MINB(R) (sizeof(R) == 8 ? 4 : 6)
 #endif
 #ifndef QCB_FLOW_THREADS
 #define QCB_FLOW_THREADS 128
@@ -241,6 +241,24 @@ struct Quat {
     double a0, a1, a2, a3;
 };
 
+// Heatbath draws ahead of use.  A subgroup update consumes Philox calls n, n+1 per Kennedy-Pendleton
+// attempt and one call for (u_phi, u_cos) after the accepted attempt, so the stream position is
+// even at every subgroup and a subgroup starting at call n needs calls n, n+1 (attempt 0) and
+// n+2 (its final draws if attempt 0 is accepted, else attempt 1's first pair).  P, Q, F hold
+// those three calls, evaluated together (independent Philox chains) before they are needed.
+struct KPDraws {
+    uint32_t n;  // first call of the current subgroup
+    double2 P, Q, F;
+};
+__device__ __forceinline__ KPDraws kp_draws_at(const LinkStream& rng, uint32_t n) {
+    KPDraws d;
+    d.n = n;
+    d.P = rng.call(n);
+    d.Q = rng.call(n + 1);
+    d.F = rng.call(n + 2);
+    return d;
+}
+
 // generate_su2_kp (src/heatbath/heatbath.cpp:8-36) + su2_step (:39-44), drawing in the
 // reference's order: (delta, r1, r2, r3) per Kennedy-Pendleton attempt, then (u_phi, u_cos).
 // With c_alpha = -0.75/beta, -0.5/alpha = c_alpha / k (alpha = 2 beta k / 3), so one rsqrt
@@ -248,19 +266,22 @@ struct Quat {
 // The loop is capped at KP_MAX_ATTEMPTS attempts and a non-finite or non-negative scale is
 // rejected up front; in either case the subgroup element is the identity (the link is left
 // unchanged by this subgroup) and the kernel raises DERR_KP_CAP.
+// `d` holds this subgroup's first draws on entry; with `more` set it holds the next subgroup's
+// on return (evaluated right after acceptance, alongside the rest of this update).
 constexpr int KP_MAX_ATTEMPTS = 4096;
-__device__ __forceinline__ Quat su2_step(double c_alpha, Quat w, LinkStream& rng, int* err) {
+__device__ __forceinline__ Quat su2_step(double c_alpha, Quat w, const LinkStream& rng, KPDraws& d, bool more,
+                                         int* err) {
     const double ik = rsqrt(w.a0 * w.a0 + w.a1 * w.a1 + w.a2 * w.a2 + w.a3 * w.a3);  // 1/k
     const Quat v = {w.a0 * ik, w.a1 * ik, w.a2 * ik, w.a3 * ik};
     const double m05a = c_alpha * ik;  // -0.5 / alpha
     double a0 = 1.0;
     bool ok = false;
     const int cap = (m05a < 0.0 && isfinite(m05a)) ? KP_MAX_ATTEMPTS : 0;
-    for (int it = 0; it < cap; it++) {
-        double delta = rng.next();
-        double r1 = rng.next();
-        double r2 = rng.next();
-        double r3 = rng.next();
+    const uint32_t n = d.n;
+    double2 P = d.P, Q = d.Q, F = d.F;
+    int it = 0;
+    for (; it < cap; it++) {
+        const double delta = P.x, r1 = P.y, r2 = Q.x, r3 = Q.y;
         double c = cospi(2.0 * r2);
         double lsq = __dmul_rn(m05a, __dadd_rn(log(r1), __dmul_rn(__dmul_rn(c, c), log(r3))));
         if (__dmul_rn(delta, delta) <= __dadd_rn(1.0, -lsq)) {
@@ -268,14 +289,21 @@ __device__ __forceinline__ Quat su2_step(double c_alpha, Quat w, LinkStream& rng
             ok = true;
             break;
         }
+        // attempt it + 1 uses calls n + 2it + 2 (= F) and n + 2it + 3
+        P = F;
+        Q = rng.call(n + 2u * (uint32_t)it + 3u);
+        F = rng.call(n + 2u * (uint32_t)it + 4u);
     }
+    // accepted at attempt it: calls n .. n + 2it + 2 are used; failed: 2 cap calls, no final draws
+    const uint32_t n_next = ok ? n + 2u * (uint32_t)it + 3u : n + 2u * (uint32_t)cap;
+    if (more) d = kp_draws_at(rng, n_next);
     if (!ok) {
         atomicOr(err, (int)DERR_KP_CAP);
         return Quat{1.0, 0.0, 0.0, 0.0};
     }
     const double rs = sqrt(1.0 - a0 * a0);
-    const double uphi = rng.next();
-    const double cos_t = 2.0 * rng.next() - 1.0;
+    const double uphi = F.x;
+    const double cos_t = 2.0 * F.y - 1.0;
     const double sin_t = sqrt(1.0 - cos_t * cos_t);
     double sp, cp;
     sincospi(2.0 * uphi, &sp, &cp);
@@ -289,8 +317,9 @@ __device__ __forceinline__ Quat su2_step(double c_alpha, Quat w, LinkStream& rng
 
 // One Cabibbo-Marinari subgroup update of u in place (src/heatbath/heatbath_mpi.cpp:14-32):
 // w = quaternion of the (I,J) block of W = u*A, r = su2_step(w), u <- embed_{IJ}(r) * u.
-template <typename R, int I, int J>
-__device__ __forceinline__ void cm_subgroup(M3<R>& u, const M3<R>& A, double c_alpha, LinkStream& rng, int* err) {
+template <typename R, int I, int J, typename AM>
+__device__ __forceinline__ void cm_subgroup(M3<R>& u, const AM& A, double c_alpha, const LinkStream& rng, KPDraws& d,
+                                            bool more, int* err) {
     Cx<R> wii = mkc<R>(0, 0), wij = mkc<R>(0, 0), wji = mkc<R>(0, 0), wjj = mkc<R>(0, 0);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -302,7 +331,7 @@ __device__ __forceinline__ void cm_subgroup(M3<R>& u, const M3<R>& A, double c_a
     // su2_to_quaternion (src/su3/utils.cpp:47-50)
     Quat w = {((double)wii.re + (double)wjj.re) / 2.0, ((double)wij.im + (double)wji.im) / 2.0,
               ((double)wij.re - (double)wji.re) / 2.0, ((double)wii.im - (double)wjj.im) / 2.0};
-    Quat r = su2_step(c_alpha, w, rng, err);
+    Quat r = su2_step(c_alpha, w, rng, d, more, err);
     // su2_quaternion_to_su3 (src/su3/utils.cpp:33-44) applied from the left
     Cx<R> rii = mkc<R>((R)r.a0, (R)r.a3), rjj = mkc<R>((R)r.a0, (R)-r.a3);
     Cx<R> rij = mkc<R>((R)r.a2, (R)r.a1), rji = mkc<R>((R)-r.a2, (R)r.a1);
@@ -318,28 +347,132 @@ __device__ __forceinline__ void cm_subgroup(M3<R>& u, const M3<R>& A, double c_a
     }
 }
 
+// A thread's staple held in shared memory for the hits: element k of the thread's matrix at
+// p[k * stride] (p offset by the thread index), so a warp touches 32 consecutive complexes per
+// element.  Reads go through ld.shared so the compiler keeps the matrix in shared memory instead
+// of forwarding it back into registers; the registers it frees raise the resident warps.
+template <typename R>
+struct StapleSlot {
+    typedef typename V2<R>::T C2;
+    C2* p;
+    int stride;
+    __device__ __forceinline__ void set(int i, int j, Cx<R> v) const {
+        const unsigned a = (unsigned)__cvta_generic_to_shared(p + (i * 3 + j) * stride);
+        if constexpr (sizeof(R) == 8)
+            asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(a), "d"(v.re), "d"(v.im) : "memory");
+        else
+            asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.re), "f"(v.im) : "memory");
+    }
+    __device__ __forceinline__ void put(const M3<R>& A) const {
+#pragma unroll
+        for (int k = 0; k < 9; k++) set(k / 3, k % 3, A.e[k]);
+    }
+    __device__ __forceinline__ Cx<R> operator()(int i, int j) const {
+        const unsigned a = (unsigned)__cvta_generic_to_shared(p + (i * 3 + j) * stride);
+        R x, y;
+        if constexpr (sizeof(R) == 8)
+            asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(x), "=d"(y) : "r"(a) : "memory");
+        else
+            asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(x), "=f"(y) : "r"(a) : "memory");
+        return mkc<R>(x, y);
+    }
+    __device__ __forceinline__ M3<R> get() const {
+        M3<R> A;
+#pragma unroll
+        for (int k = 0; k < 9; k++) A.e[k] = (*this)(k / 3, k % 3);
+        return A;
+    }
+};
+
+// cm_subgroup with the link and the staple in shared-memory slots and the subgroup (I, J) chosen
+// at run time: one copy of the update code serves the three subgroups of a hit.
+template <typename R>
+__device__ __forceinline__ void cm_subgroup_rt(const StapleSlot<R>& u, const StapleSlot<R>& A, int I, int J,
+                                               double c_alpha, const LinkStream& rng, KPDraws& d, bool more,
+                                               int* err) {
+    Cx<R> ui[3], uj[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        ui[k] = u(I, k);
+        uj[k] = u(J, k);
+    }
+    Cx<R> wii = mkc<R>(0, 0), wij = mkc<R>(0, 0), wji = mkc<R>(0, 0), wjj = mkc<R>(0, 0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const Cx<R> aki = A(k, I), akj = A(k, J);
+        cmac(wii, ui[k], aki);
+        cmac(wij, ui[k], akj);
+        cmac(wji, uj[k], aki);
+        cmac(wjj, uj[k], akj);
+    }
+    Quat w = {((double)wii.re + (double)wjj.re) / 2.0, ((double)wij.im + (double)wji.im) / 2.0,
+              ((double)wij.re - (double)wji.re) / 2.0, ((double)wii.im - (double)wjj.im) / 2.0};
+    Quat r = su2_step(c_alpha, w, rng, d, more, err);
+    Cx<R> rii = mkc<R>((R)r.a0, (R)r.a3), rjj = mkc<R>((R)r.a0, (R)-r.a3);
+    Cx<R> rij = mkc<R>((R)r.a2, (R)r.a1), rji = mkc<R>((R)-r.a2, (R)r.a1);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        Cx<R> ni = rii * ui[k];
+        cmac(ni, rij, uj[k]);
+        Cx<R> nj = rji * ui[k];
+        cmac(nj, rjj, uj[k]);
+        u.set(I, k, ni);
+        u.set(J, k, nj);
+    }
+}
+
 // Heatbath update of one link (x, mu) of the (parity, mu) set being swept: no link of the set
 // appears in another's staple, so all links of the set update concurrently.  Replaces
 // mpi::heatbathcb::hit / sweep (heatbath_mpi.cpp:10-57) for one link; the staple is computed
 // once per link, since it does not contain U(x,mu) and is therefore identical for every hit
-// (the reference recomputes it per hit).  MU >= 0 selects the direction at compile time.
-template <typename R, int NE, int MU>
+// (the reference recomputes it per hit).  The staple uses two-row products (staple_rt_rows);
+// for FP64 the rebuilt third rows differ from explicit products by the links' distance from
+// SU(3) (~1e-15), well inside the 1e-12 parity bound.
+//
+// With a shared-memory slot (SLOT = true: 18 complexes per thread at slot[k * slot_stride]) the
+// staple and the link live in the slot during the hits and one rolled copy of the subgroup update
+// serves all 3 * n_hits updates (cm_subgroup_rt): the hit code is a third of the unrolled size
+// and needs few registers.  Without a slot (blocks too large for the static shared memory) the
+// three subgroups are unrolled on register-resident matrices.
+template <typename R, int NE, int MU, bool SLOT>
 __device__ __forceinline__ void hb_link(const Geom& g, const LinkField<R, NE>& U, int par, int h, double c_alpha,
-                                        int n_hits, uint64_t seed, uint32_t sweep, int reproject, int* err) {
+                                        int n_hits, uint64_t seed, uint32_t sweep, int reproject, int* err,
+                                        typename V2<R>::T* slot, int slot_stride) {
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
     const int lex = lex_of(g, c);
-    M3<R> A = staple<R, NE, MU, true>(g, U, c, lex, par);
-    M3<R> u = U.load(MU, par, h);
-    LinkStream rng(seed, (uint32_t)(lex * 4 + MU), sweep, TAG_HB);
-    for (int hit = 0; hit < n_hits; hit++) {
-        cm_subgroup<R, 0, 1>(u, A, c_alpha, rng, err);
-        cm_subgroup<R, 1, 2>(u, A, c_alpha, rng, err);
-        cm_subgroup<R, 0, 2>(u, A, c_alpha, rng, err);
+    const M3<R> A = staple_rt_rows<R, NE>(g, U, c, lex, par, MU);
+    const LinkStream rng(seed, (uint32_t)(lex * 4 + MU), sweep, TAG_HB);
+    KPDraws d = kp_draws_at(rng, 0u);
+    M3<R> u;
+    if constexpr (SLOT) {
+        const StapleSlot<R> S{slot, slot_stride}, Us{slot + 9 * slot_stride, slot_stride};
+        S.put(A);
+        Us.put(U.load(MU, par, h));
+        const int n_sub = 3 * n_hits;
+#pragma unroll 1
+        for (int it = 0; it < n_sub; it++) {
+            const int sg = it - 3 * (it / 3);  // subgroups (0,1), (1,2), (0,2) in turn
+            cm_subgroup_rt<R>(Us, S, sg == 1 ? 1 : 0, sg == 0 ? 1 : 2, c_alpha, rng, d, it + 1 < n_sub, err);
+        }
+        u = Us.get();
+    } else {
+        u = U.load(MU, par, h);
+        for (int hit = 0; hit < n_hits; hit++) {
+            cm_subgroup<R, 0, 1>(u, A, c_alpha, rng, d, true, err);
+            cm_subgroup<R, 1, 2>(u, A, c_alpha, rng, d, true, err);
+            cm_subgroup<R, 0, 2>(u, A, c_alpha, rng, d, hit + 1 < n_hits, err);
+        }
     }
     if (reproject) reproject_fp64(u);
     U.store(MU, par, h, u);
 }
+
+// Shared-memory slot of a heatbath block: 18 complexes per thread (staple and link).
+template <typename R, int BLOCK>
+struct HbSlotFits {
+    static constexpr bool value = 18 * BLOCK * sizeof(typename V2<R>::T) <= 48 * 1024;
+};
 
 // Single-lattice heatbath launch: one thread per link of the (par, MU) set, geometry as kernel
 // parameters.
@@ -349,7 +482,10 @@ __global__ void __launch_bounds__(QCB_HB_THREADS, QCB_HB_MINB(R))
                   int reproject, int* err) {
     const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= g.Vh) return;
-    hb_link<R, NE, MU>(g, U, par, (int)h, c_alpha, n_hits, seed, sweep, reproject, err);
+    static_assert(HbSlotFits<R, QCB_HB_THREADS>::value, "heatbath slot exceeds static shared memory");
+    __shared__ typename V2<R>::T slot[18 * QCB_HB_THREADS];
+    hb_link<R, NE, MU, true>(g, U, par, (int)h, c_alpha, n_hits, seed, sweep, reproject, err, slot + threadIdx.x,
+                             QCB_HB_THREADS);
 }
 
 // ------------------------------------------------------------------ Wilson flow

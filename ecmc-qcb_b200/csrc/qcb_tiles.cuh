@@ -53,14 +53,17 @@ __global__ void __launch_bounds__(BLOCK, MINB)
                int par, int n_hits, const uint32_t* sweep_dev, uint32_t sweep_add, int reproject, int* err) {
     const uint32_t sweep = sweep_add + (sweep_dev ? *sweep_dev : 0u);
     const int64_t total = (int64_t)ntiles * TILE;
+    constexpr bool SLOT = HbSlotFits<R, BLOCK>::value;
+    __shared__ typename V2<R>::T slot[(SLOT ? 18 : 1) * BLOCK];
+    typename V2<R>::T* my = slot + threadIdx.x;
     for (int64_t v = (int64_t)blockIdx.x * BLOCK + threadIdx.x; v < total; v += (int64_t)gridDim.x * BLOCK) {
         const int tile = (int)(v / TILE);
         const LatDesc* d = lattice_of(lats, tile_lat, one, tile);
         const Geom g = d->g;
         const int h = (tile - d->nb_begin) * TILE + (int)(v % TILE);
         if (h < g.Vh)
-            hb_link<R, NE, MU>(g, lview<R, NE>(d->links, g.Vh), par, h, d->c_alpha, n_hits, d->seed, sweep,
-                               reproject, err);
+            hb_link<R, NE, MU, SLOT>(g, lview<R, NE>(d->links, g.Vh), par, h, d->c_alpha, n_hits, d->seed, sweep,
+                                     reproject, err, my, BLOCK);
     }
 }
 
