@@ -349,10 +349,11 @@ def run_batch(qcb):
             "launches_per_sweep": 9, "graph": True}
 
 
-def run_serve(qcb, n_req: int):
+def run_serve(qcb, n_req: int, store: int = 1):
     """Serving: Poisson arrivals at 100 req/s, L in {8,12,16,20,24,32} with p = (.3,.25,.2,.1,.1,.05),
     beta ~ U[5.8, 6.3], inputs = 50 FP64 sweeps from seed = request id (excluded from latency), flow
-    eps = 0.02 to t = L^2/32 in FP32 with Q/E every step; against one-at-a-time plain FP64 flow."""
+    eps = 0.02 to t = L^2/32 in FP32 links (12-real storage by default) with FP64 reprojection and
+    Q/E every step; against one-at-a-time plain FP64 flow."""
     import numpy as np
 
     rng = np.random.default_rng(2026)
@@ -366,7 +367,7 @@ def run_serve(qcb, n_req: int):
     b.close()
     steps = [int(round(x * x / 32 / 0.02)) + 1 for x in sizes]
     site_steps = sum(int(x) ** 4 * (n - 1) for x, n in zip(sizes, steps))
-    srv = qcb.Server(150 << 30, prec=qcb.PREC_F32, store=qcb.STORE_18)
+    srv = qcb.Server(150 << 30, prec=qcb.PREC_F32, store=store)
     time.sleep(FLOW_COOL_S)  # both arms start from an idle GPU
     start = srv.now()
     k, done = 0, {}
@@ -399,7 +400,8 @@ def run_serve(qcb, n_req: int):
         fl.close()
         f.close()
     lat2 = np.array(lat2)
-    return {"requests": n_req, "rate_per_s": 100.0, "site_steps": site_steps, "prec": "fp32-18",
+    return {"requests": n_req, "rate_per_s": 100.0, "site_steps": site_steps,
+            "prec": "fp32-12" if store == 1 else "fp32-18",
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "configs_per_s": n_req / wall, "site_steps_per_s": site_steps / wall,
             "peak_resident": st["peak_resident"], "peak_bytes": st["peak_bytes"],

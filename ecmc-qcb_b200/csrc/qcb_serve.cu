@@ -5,10 +5,13 @@
 //   * admission: requests leave the FIFO in order as soon as the HBM budget (and the active
 //     limit) leaves room for their flowed field, RK3 buffers and measurements; memory comes from
 //     the server's own stream-ordered pool and returns to it when a request completes;
-//   * one scheduler tick measures Q/E of every resident request (one batched clover launch and
-//     one per-request finalize) and then advances every resident request by n_rk RK3 steps with
-//     three persistent launches per step over the tile work list of all of them, so requests
-//     that arrive while others are on the GPU share the same launches;
+//   * one scheduler tick measures Q/E of every resident request and then advances every
+//     resident request by n_rk RK3 steps.  Requests below kBigVh half-sites share one batched
+//     clover launch (with a per-request finalize) and three persistent launches per RK3 step over
+//     the tile work list of all of them, so requests that arrive while others are on the GPU
+//     share the same launches; a request of kBigVh half-sites or more fills the GPU by itself and
+//     runs the single-lattice kernels (geometry in kernel parameters, no per-tile descriptor
+//     lookups), in the same stream between the shared launches;
 //   * a request that has taken its last measurement is copied back, frees its memory and is
 //     handed to qcb_serve_poll with its submit and completion times.
 // Per-request results do not depend on the other requests in the mix: every link and every
@@ -52,6 +55,11 @@ struct Request {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Requests with at least this many half-sites (L >= 24 for L^4) run their own single-lattice
+// launches; the choice depends on the request alone, so its result does not depend on the mix.
+constexpr int64_t kBigVh = (int64_t)1 << 17;
+bool is_big(const Request* r) { return r->g.Vh >= kBigVh; }
+
 }  // namespace
 
 struct qcb_server_s {
@@ -62,6 +70,9 @@ struct qcb_server_s {
     std::condition_variable cv_work, cv_done;
     std::deque<Request*> pending, done;
     std::vector<Request*> active;
+    std::vector<Request*> small, big;  // the active set split by size (rebuild)
+    double* big_partials = nullptr;
+    size_t big_partials_cap = 0;
     size_t bytes_in_use = 0, bytes_peak = 0;
     uint64_t submitted = 0, completed = 0;
     bool stop = false;
@@ -94,7 +105,8 @@ struct qcb_server_s {
 namespace {
 
 // Per-request deterministic sums of clover partials, stored in the request's slot of this tick:
-// meas[(tick - tick0) * 2 + k] = (Q, sum e).
+// meas[(tick - tick0) * 3 + k] = (Q, sum e) (k = 0, 1; slot k = 2 is the plaquette sum, which
+// only the single-lattice path measures).
 __global__ void k_meas_finalize(const LatDesc* __restrict__ lats, const double* __restrict__ partials, int tick) {
     __shared__ double sm[256];
     const LatDesc* d = lats + blockIdx.x;
@@ -108,7 +120,7 @@ __global__ void k_meas_finalize(const LatDesc* __restrict__ lats, const double* 
             if ((int)threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
             __syncthreads();
         }
-        if (threadIdx.x == 0) d->meas[(size_t)(tick - d->tick0) * 2 + k] = sm[0];
+        if (threadIdx.x == 0) d->meas[(size_t)(tick - d->tick0) * 3 + k] = sm[0];
         __syncthreads();
     }
 }
@@ -144,10 +156,13 @@ bool grow(qcb_server_s* s, T** p, size_t* cap, size_t n) {
 // Rebuilds the descriptors and tile map of the active set.
 bool rebuild(qcb_server_s* s) {
     s->desc.clear();
+    s->small.clear();
+    s->big.clear();
+    for (Request* r : s->active) (is_big(r) ? s->big : s->small).push_back(r);
     std::vector<int> tile_lat;
     int nb = 0;
-    for (size_t i = 0; i < s->active.size(); i++) {
-        Request* r = s->active[i];
+    for (size_t i = 0; i < s->small.size(); i++) {
+        Request* r = s->small[i];
         LatDesc d;
         memset(&d, 0, sizeof(d));
         d.g = r->g;
@@ -194,7 +209,7 @@ bool admit(qcb_server_s* s, Request* r) {
 }
 
 bool finish(qcb_server_s* s, Request* r) {
-    std::vector<double> meas((size_t)r->n_steps * 2);
+    std::vector<double> meas((size_t)r->n_steps * 3);
     if (!cuda_ok(s, cudaMemcpyAsync(meas.data(), (char*)r->buf + r->off_meas, meas.size() * sizeof(double),
                                     cudaMemcpyDeviceToHost, s->stream), "result readback"))
         return false;
@@ -205,12 +220,46 @@ bool finish(qcb_server_s* s, Request* r) {
     double t = 0.0;
     for (int k = 0; k < r->n_steps; k++) {
         r->tqe[3 * k] = t;
-        r->tqe[3 * k + 1] = meas[2 * k];
-        r->tqe[3 * k + 2] = meas[2 * k + 1] / (double)r->g.V;
+        r->tqe[3 * k + 1] = meas[3 * k];
+        r->tqe[3 * k + 2] = meas[3 * k + 1] / (double)r->g.V;
         for (int j = 0; j < s->n_rk; j++) t += r->eps;
     }
     r->t_done = s->now();
     return true;
+}
+
+// Current links of a request: buffer A when an even number of RK3 steps has run since its
+// admission, else buffer B (the rule the tiled kernels apply through flip ^ flip_xor).
+void* current_links(const Request* r, int flip_xor) {
+    return ((r->flip ^ flip_xor) & 1) ? (char*)r->buf + r->off_out : r->buf;
+}
+
+// Clover Q/E (and plaquette) of a big request with the single-lattice kernel, summed into its
+// measurement slot of this tick.
+bool measure_big(qcb_server_s* s, Request* r, int flip_xor) {
+    const int64_t need = (r->g.Vh + 127) / 128;
+    const unsigned nbx = (unsigned)std::min<int64_t>(need, 148 * 8);
+    if (!grow(s, &s->big_partials, &s->big_partials_cap, (size_t)nbx * 6 * 3)) return false;
+    if (!cuda_ok(s, fmt_ops(s->fmt).clover(r->g, current_links(r, flip_xor), s->big_partials, nbx, s->stream),
+                 "clover launch"))
+        return false;
+    double* slot = (double*)((char*)r->buf + r->off_meas) + (size_t)(s->tick - r->tick0) * 3;
+    k_finalize<<<1, 256, 0, s->stream>>>(s->big_partials, (int)(nbx * 6), 3, 0u, slot);
+    note_launches(2);
+    return cuda_ok(s, cudaGetLastError(), "measure finalize");
+}
+
+// One RK3 stage of a big request: stage s reads buffer A when (f + s - 1) is even (f = number
+// of RK3 steps since admission, mod 2) and writes the other buffer.
+bool flow_big(qcb_server_s* s, Request* r, int stage, int flip_xor, int rep) {
+    const int f = (r->flip ^ flip_xor) & 1;
+    void* a = r->buf;
+    void* b = (char*)r->buf + r->off_out;
+    const bool in_b = ((f + stage - 1) & 1) != 0;
+    note_launches(1);
+    return cuda_ok(s, fmt_ops(s->fmt).flow1(r->g, in_b ? b : a, in_b ? a : b, (char*)r->buf + r->off_z, r->eps, stage,
+                                            rep, s->stream),
+                   "flow launch");
 }
 
 void scheduler(qcb_server_s* s) {
@@ -245,12 +294,16 @@ void scheduler(qcb_server_s* s) {
         w.lats = s->d_desc;
         w.tile_lat = s->d_tile_lat;
         w.nb_total = s->nb_total;
-        w.nlat = (int)s->active.size();
+        w.nlat = (int)s->small.size();
         const int fx = (int)(s->nflow & 1);
-        if (!cuda_ok(s, fmt_ops(s->fmt).clover_tiles(w, fx, s->partials, s->stream), "clover launch")) break;
-        k_meas_finalize<<<(unsigned)s->active.size(), 256, 0, s->stream>>>(s->d_desc, s->partials, s->tick);
-        if (!cuda_ok(s, cudaGetLastError(), "measure finalize")) break;
-        note_launches(2);
+        if (!s->small.empty()) {
+            if (!cuda_ok(s, fmt_ops(s->fmt).clover_tiles(w, fx, s->partials, s->stream), "clover launch")) break;
+            k_meas_finalize<<<(unsigned)s->small.size(), 256, 0, s->stream>>>(s->d_desc, s->partials, s->tick);
+            if (!cuda_ok(s, cudaGetLastError(), "measure finalize")) break;
+            note_launches(2);
+        }
+        for (Request* r : s->big) ok = ok && measure_big(s, r, fx);
+        if (!ok) break;
         // requests that took their last measurement leave the mix
         std::vector<Request*> leaving, staying;
         for (Request* r : s->active) (s->tick - r->tick0 == r->n_steps - 1 ? leaving : staying).push_back(r);
@@ -263,13 +316,17 @@ void scheduler(qcb_server_s* s) {
             w.lats = s->d_desc;
             w.tile_lat = s->d_tile_lat;
             w.nb_total = s->nb_total;
-            w.nlat = (int)s->active.size();
+            w.nlat = (int)s->small.size();
         }
         for (int k = 0; k < s->n_rk && !s->active.empty() && ok; k++) {
             const int f = (int)(s->nflow & 1);
-            for (int stage = 1; stage <= 3 && ok; stage++)
-                ok = cuda_ok(s, fmt_ops(s->fmt).flow(w, stage, f, rep, s->stream), "flow launch");
-            note_launches(3);
+            for (int stage = 1; stage <= 3 && ok; stage++) {
+                if (!s->small.empty()) {
+                    ok = cuda_ok(s, fmt_ops(s->fmt).flow(w, stage, f, rep, s->stream), "flow launch");
+                    note_launches(1);
+                }
+                for (Request* r : s->big) ok = ok && flow_big(s, r, stage, f, rep);
+            }
             s->nflow++;
         }
         if (!ok) break;
@@ -349,6 +406,7 @@ int qcb_serve_destroy(qcb_server s) {
     if (s->d_desc) cudaFree(s->d_desc);
     if (s->d_tile_lat) cudaFree(s->d_tile_lat);
     if (s->partials) cudaFree(s->partials);
+    if (s->big_partials) cudaFree(s->big_partials);
     if (s->staging) cudaFree(s->staging);
     if (s->pool) cudaMemPoolDestroy(s->pool);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -377,7 +435,7 @@ int qcb_serve_submit(qcb_server s, uint64_t id, const int L[4], const double* li
     r->off_out = lb;
     r->off_z = 2 * lb;
     r->off_meas = 2 * lb + align256(alg_bytes(s->fmt, r->g.Vh));
-    r->bytes = r->off_meas + align256((size_t)n_steps * 2 * sizeof(double));
+    r->bytes = r->off_meas + align256((size_t)n_steps * 3 * sizeof(double));
     if (r->bytes > s->budget) {
         delete r;
         return fail(QCB_ENOMEM, "serve submit: request needs %zu bytes, budget is %zu", r->bytes, s->budget);

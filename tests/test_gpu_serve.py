@@ -104,3 +104,20 @@ def test_server_errors(gpu):
     assert e.value.code == -6
     s2.wait(300.0)
     assert s2.poll()[0] == 9
+
+
+def test_big_request_single_lattice_path(gpu):
+    """A request of 2^17 half-sites or more (here 24^4) runs the single-lattice kernels: its result is
+    bit-identical to the plain measured flow and the same alone and next to small requests."""
+    f, U = config(gpu, (24,) * 4, 31, sweeps=1)
+    s = gpu.Server(8 << 30, prec=32)
+    alone = run(s, [(1, f.L, U, 4)])[1][1]
+    s.close()
+    fl = gpu.GradientFlow(f, EPS, prec=32, store=0)
+    ref = fl.measure(f, 4, 1)
+    assert np.array_equal(alone, ref)
+    g, Ug = config(gpu, (8,) * 4, 32)
+    s = gpu.Server(8 << 30, prec=32)
+    mix = run(s, [(1, f.L, U, 4), (2, g.L, Ug, 6), (3, g.L, Ug, 3)])
+    assert np.array_equal(mix[1][1], alone)
+    assert s.stats()["peak_resident"] >= 2
