@@ -302,6 +302,34 @@ def flow_accuracy(qcb, src, n_steps):
     return out
 
 
+def run_precision(qcb, n_therm: int = 500, n_flow: int = 400):
+    """The precision configuration at full size: 48^4, beta = 6.2, hot start from seed 99 and
+    n_therm FP64 heatbath sweeps (N_hits = 2), then the flow eps = 0.02 for n_flow steps (t = 8.0)
+    measured at every step in FP64 and in FP32 (18 and 12 reals); max |dQ(t)|, dE(t)/E(t) and
+    dP(t) over all n_flow + 1 measurements against the FP64 flow."""
+    Lp = (48, 48, 48, 48)
+    f = qcb.GaugeField(Lp, qcb.PREC_F64, qcb.STORE_18)
+    f.hot_start(99)
+    for k in range(n_therm):
+        f.hb_sweep(6.2, N_HITS, 99, k)
+    plaq = f.plaquette()
+    ref = qcb.GradientFlow(f, 0.02, prec=64, store=0)
+    t64, p64 = ref.measure(f, n_flow + 1, 1, plaquette=True)
+    ref.close()
+    out = {"L": list(Lp), "beta": 6.2, "therm_sweeps": n_therm, "n_hits": N_HITS, "plaquette_therm": plaq,
+           "flow_steps": n_flow, "t_final": float(t64[-1, 0]), "Q_final_fp64": float(t64[-1, 1]),
+           "E_final_fp64": float(t64[-1, 2])}
+    for store, tag in ((0, "fp32_18"), (1, "fp32_12")):
+        fl = qcb.GradientFlow(f, 0.02, prec=32, store=store)
+        t32, p32 = fl.measure(f, n_flow + 1, 1, plaquette=True)
+        fl.close()
+        out[tag] = {"dQ_max": float(max(abs(t32[:, 1] - t64[:, 1]))),
+                    "dE_rel_max": float(max(abs(t32[:, 2] - t64[:, 2]) / abs(t64[:, 2]))),
+                    "dP_max": float(max(abs(p32 - p64)))}
+    f.close()
+    return out
+
+
 def run_batch(qcb):
     """Batched chains: 96x8^4 + 96x12^4 + 48x16^4 + 16x24^4, beta ~ U[5.7, 6.3], seeds 0..255, hot
     starts, FP64; autotuned, CUDA-graph sweeps; against the same sweeps run chain by chain."""
@@ -515,6 +543,7 @@ def run_ours(args, rank: int, world: int, local: int):
                                      "frac": ach / hbm_peak}}
         g.close()
 
+    precision = run_precision(qcb) if args.parts in ("all",) else None
     batch = run_batch(qcb) if args.parts in ("all",) else None
     serve = run_serve(qcb, args.serve_requests) if args.parts in ("all",) else None
 
@@ -545,6 +574,7 @@ def run_ours(args, rank: int, world: int, local: int):
             "plaquette_after": plaq,
             "hb": hb_more,
             "flow": flow,
+            "precision": precision,
             "batch": batch,
             "serve": serve,
         }
