@@ -141,8 +141,7 @@ __device__ __forceinline__ M3<R> staple_rt_rows(const Geom& g, const LinkField<R
 #pragma unroll
             for (int j = 0; j < 3; j++) {
                 const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
-                cmac_cc(A(2, j), s[0][j1], s[1][j2]);
-                cmac_cc(A(2, j), mkc<R>(-s[0][j2].re, -s[0][j2].im), s[1][j1]);
+                A(2, j) = A(2, j) + conj_cross(s[0][j1], s[1][j2], s[0][j2], s[1][j1]);
             }
         }
         {
@@ -170,8 +169,7 @@ __device__ __forceinline__ M3<R> staple_rt_rows(const Geom& g, const LinkField<R
 #pragma unroll
             for (int j = 0; j < 3; j++) {
                 const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
-                cmac_cc(A(2, j), s[0][j1], s[1][j2]);
-                cmac_cc(A(2, j), mkc<R>(-s[0][j2].re, -s[0][j2].im), s[1][j1]);
+                A(2, j) = A(2, j) + conj_cross(s[0][j1], s[1][j2], s[0][j2], s[1][j1]);
             }
         }
     }
@@ -212,8 +210,8 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
 }
 
 // Launch shapes (measured on B200, 32^4): 128-thread blocks.  Minimum resident blocks per SM:
-// heatbath 4 for FP64 (<= 128 registers; 0.236 ms a sub-sweep at N_hits = 2 against 0.245 ms at
-// 3) and 6 for FP32; flow stages 3 for FP64 (<= 168 registers; 4 is no faster) and 6 for FP32
+// heatbath 4 for FP64 (<= 128 registers; 0.217 ms a sub-sweep at N_hits = 2 against 0.224 ms at
+// 5 and 0.259 ms at 6) and 6 for FP32; flow stages 3 for FP64 (<= 168 registers; 4 is no faster) and 6 for FP32
 // (<= 80 registers, no spills: 0.36 ms a stage against 0.40 ms at 4 and 0.37 ms at 8).
 #ifndef QCB_HB_THREADS
 #define QCB_HB_THREADS 128
@@ -384,6 +382,83 @@ struct StapleSlot {
     }
 };
 
+// staple_rt_rows accumulated into a shared-memory slot instead of registers: each forward or
+// backward staple is formed in registers and added to the slot, so the 18-real accumulator does not
+// occupy registers across the nu loop.
+template <typename R, int NE>
+__device__ __forceinline__ void staple_rows_into(const Geom& g, const LinkField<R, NE>& U, const int c[4], int lex,
+                                                 int par, int mu, const StapleSlot<R>& S) {
+#pragma unroll
+    for (int e = 0; e < 9; e++) S.set(e / 3, e % 3, mkc<R>(0, 0));
+    const int opp = par ^ 1;
+    const Steps st = make_steps(g, c);
+    const int xmu = lex + sel4(st.up, mu);
+    auto add_rows = [&](const Cx<R> r[2][3]) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+            const Cx<R> r2 = conj_cross(r[0][j1], r[1][j2], r[0][j2], r[1][j1]);
+            S.set(0, j, S(0, j) + r[0][j]);
+            S.set(1, j, S(1, j) + r[1][j]);
+            S.set(2, j, S(2, j) + r2);
+        }
+    };
+#pragma unroll 1
+    for (int k = 0; k < 3; k++) {
+        const int nu = k < mu ? k : k + 1;
+        const int dnu = sel4(st.dn, nu);
+        const int xnu = lex + sel4(st.up, nu);
+        const int xmnu = lex + dnu;
+        const int xmumnu = xmu + dnu;
+        {
+            const M3<R> a = U.load_ro(nu, opp, xmu >> 1);
+            const M3<R> b = U.load_ro(mu, opp, xnu >> 1);
+            Cx<R> t[2][3], r[2][3];
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    t[i][j] = mkc<R>(0, 0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) cmac_nc(t[i][j], a(i, q), b(j, q));
+                }
+            const M3<R> d = U.load_ro(nu, par, lex >> 1);
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    r[i][j] = mkc<R>(0, 0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) cmac_nc(r[i][j], t[i][q], d(j, q));
+                }
+            add_rows(r);
+        }
+        {
+            const M3<R> v1 = U.load_ro(mu, opp, xmnu >> 1);
+            const M3<R> v0 = U.load_ro(nu, par, xmumnu >> 1);
+            Cx<R> t[3][2], r[2][3];
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    t[i][j] = mkc<R>(0, 0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) cmac(t[i][j], v1(i, q), v0(q, j));
+                }
+            const M3<R> v2 = U.load_ro(nu, opp, xmnu >> 1);
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    r[i][j] = mkc<R>(0, 0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) cmac_cn(r[i][j], t[q][i], v2(q, j));
+                }
+            add_rows(r);
+        }
+    }
+}
+
 // cm_subgroup with the link and the staple in shared-memory slots and the subgroup (I, J) chosen
 // at run time: one copy of the update code serves the three subgroups of a hit.
 template <typename R>
@@ -430,10 +505,12 @@ __device__ __forceinline__ void cm_subgroup_rt(const StapleSlot<R>& u, const Sta
 // SU(3) (~1e-15), well inside the 1e-12 parity bound.
 //
 // With a shared-memory slot (SLOT = true: 18 complexes per thread at slot[k * slot_stride]) the
-// staple and the link live in the slot during the hits and one rolled copy of the subgroup update
-// serves all 3 * n_hits updates (cm_subgroup_rt): the hit code is a third of the unrolled size
-// and needs few registers.  Without a slot (blocks too large for the static shared memory) the
-// three subgroups are unrolled on register-resident matrices.
+// staple is accumulated in the slot (staple_rows_into), the link joins it there, and one rolled
+// copy of the subgroup update serves all 3 * n_hits updates (cm_subgroup_rt): the hit code is a
+// third of the unrolled size and neither phase keeps a 3x3 accumulator in registers (0.217 ms a
+// 32^4 FP64 sub-sweep at N_hits = 2 against 0.235 ms with the staple in registers).  Without a
+// slot (blocks too large for the static shared memory) the three subgroups are unrolled on
+// register-resident matrices.
 template <typename R, int NE, int MU, bool SLOT>
 __device__ __forceinline__ void hb_link(const Geom& g, const LinkField<R, NE>& U, int par, int h, double c_alpha,
                                         int n_hits, uint64_t seed, uint32_t sweep, int reproject, int* err,
@@ -441,13 +518,12 @@ __device__ __forceinline__ void hb_link(const Geom& g, const LinkField<R, NE>& U
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
     const int lex = lex_of(g, c);
-    const M3<R> A = staple_rt_rows<R, NE>(g, U, c, lex, par, MU);
     const LinkStream rng(seed, (uint32_t)(lex * 4 + MU), sweep, TAG_HB);
-    KPDraws d = kp_draws_at(rng, 0u);
     M3<R> u;
     if constexpr (SLOT) {
         const StapleSlot<R> S{slot, slot_stride}, Us{slot + 9 * slot_stride, slot_stride};
-        S.put(A);
+        staple_rows_into<R, NE>(g, U, c, lex, par, MU, S);
+        KPDraws d = kp_draws_at(rng, 0u);
         Us.put(U.load(MU, par, h));
         const int n_sub = 3 * n_hits;
 #pragma unroll 1
@@ -457,6 +533,8 @@ __device__ __forceinline__ void hb_link(const Geom& g, const LinkField<R, NE>& U
         }
         u = Us.get();
     } else {
+        const M3<R> A = staple_rt_rows<R, NE>(g, U, c, lex, par, MU);
+        KPDraws d = kp_draws_at(rng, 0u);
         u = U.load(MU, par, h);
         for (int hit = 0; hit < n_hits; hit++) {
             cm_subgroup<R, 0, 1>(u, A, c_alpha, rng, d, true, err);

@@ -439,6 +439,15 @@ QCB_HD void reproject_fp64(M3<R>& U) {
     }
 }
 
+// conj(a b - c d) with a fixed sequence of fused multiply-adds, so that every staple routine that
+// rebuilds a third row rounds it identically.
+template <typename R>
+QCB_HD Cx<R> conj_cross(Cx<R> a, Cx<R> b, Cx<R> c, Cx<R> d) {
+    const R re = fma(a.re, b.re, fma(-a.im, b.im, fma(-c.re, d.re, c.im * d.im)));
+    const R im = fma(a.re, b.im, fma(a.im, b.re, fma(-c.re, d.im, -(c.im * d.re))));
+    return mkc<R>(re, -im);
+}
+
 // Third row of an SU(3) matrix from its first two: r2 = conj(r0 x r1).
 template <typename R>
 QCB_HD void rebuild_row2(M3<R>& U) {
