@@ -143,7 +143,8 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(n_gpus: int):
+def dist_setup(n_gpus: int, backend: str | None = None):
+    """One process per GPU (torchrun's RANK / WORLD_SIZE / LOCAL_RANK): NCCL on GPUs, gloo on CPU."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -152,8 +153,10 @@ def dist_setup(n_gpus: int):
         import torch.distributed as dist
         from datetime import timedelta
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
     return rank, world, local
 
 
@@ -170,9 +173,15 @@ def max_over_ranks(x: float, world: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_rate(units_per_rank: float, ms_max: float, world: int) -> float:
+    """Whole-job rate of `world` independent replicas (weak scaling): all ranks' units over the
+    slowest rank's time."""
+    return world * units_per_rank / (ms_max * 1e-3)
 
 
 def cuda_timer(qcb, field):
@@ -478,7 +487,7 @@ def run_ours(args, rank: int, world: int, local: int):
     n_hb, hb_ms = f.timing_read(qcb.K_HB)
     f.timing(False)
     link_upd = 4 * V * args.steps
-    value = world * link_upd / (ms * 1e-3)
+    value = replica_rate(link_upd, ms, world)
     per_launch_ms = hb_ms / n_hb
     bytes_launch = 9 * S_U[64] * (V // 2)  # 9 s_U per link-update, V/2 link-updates per (parity, mu) launch
     achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9
@@ -508,7 +517,7 @@ def run_ours(args, rank: int, world: int, local: int):
     eb.record(es)
     eb.synchronize()
     e2e_ms = max_over_ranks(ea.elapsed_time(eb), world)
-    e2e_value = world * 4 * V * n_e2e / (e2e_ms * 1e-3)
+    e2e_value = replica_rate(4 * V * n_e2e, e2e_ms, world)
     e2e_f.close()
     del U_host
 

@@ -1,0 +1,67 @@
+"""bench.py --gpus N runs independent replicas (one lattice per rank, no data-path collective): the
+rank plumbing it uses -- process-group set-up, barrier, max-over-ranks timing, the weak-scaling
+aggregate and the reference arm's rank-0-only rule -- exercised as two gloo ranks on the CPU, each
+advancing its own seeded lattice with the CPU restatement."""
+import multiprocessing as mp
+import os
+import socket
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank), MASTER_ADDR="127.0.0.1",
+                      MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    import bench
+    import torch.distributed as dist
+
+    r, w, _ = bench.dist_setup(world, backend="gloo")
+    orc = bench.load_oracle()
+    orc.set_threads(1)
+    L = (4, 4, 4, 4)
+    U = orc.hot_start(L, 100 + r)  # each replica its own seed
+    orc.hb_sweep(U, L, 6.0, 1, 100 + r, 0)
+    ms = 10.0 * (r + 1)  # per-rank "duration": the job time is the slowest rank's
+    bench.barrier(w)
+    mx = bench.max_over_ranks(ms, w)
+    out.put((r, w, mx, orc.plaquette(U, L), bench.replica_rate(1000.0, mx, w)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_replicas():
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(out.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [x[0] for x in res] == [0, 1] and all(x[1] == 2 for x in res)
+    assert all(x[2] == 20.0 for x in res)  # max over ranks on every rank
+    assert res[0][3] != res[1][3]  # independent replicas
+    assert all(x[4] == pytest.approx(2 * 1000.0 / 0.020) for x in res)
+
+
+def test_reference_arm_runs_on_rank_zero_only(capsys):
+    sys.path.insert(0, ROOT)
+    import bench
+
+    class Args:
+        steps, warmup, gpus = 1, 0, 2
+
+    assert bench.run_reference(Args, rank=1, world=2) is None
+    assert capsys.readouterr().out == ""
