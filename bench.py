@@ -339,9 +339,12 @@ def run_precision(qcb, n_therm: int = 500, n_flow: int = 400):
     return out
 
 
-def run_batch(qcb):
-    """Batched chains: 96x8^4 + 96x12^4 + 48x16^4 + 16x24^4, beta ~ U[5.7, 6.3], seeds 0..255, hot
-    starts, FP64; autotuned, CUDA-graph sweeps; against the same sweeps run chain by chain."""
+def run_batch(qcb, n_sweeps: int = 300):
+    """Batched chains (the batching configuration): 96x8^4 + 96x12^4 + 48x16^4 + 16x24^4, beta ~
+    U[5.7, 6.3], seeds 0..255, hot starts, FP64, N_hits = 1; launch shape and storage autotuned on
+    the live batch, then n_sweeps CUDA-graph sweeps timed.  Per-chain <P> of one chain of each size
+    is checked against a separate single-chain run of the same seed, storage and sweeps; the
+    speed-up is against the same sweeps run chain by chain."""
     import numpy as np
     import torch
 
@@ -351,17 +354,35 @@ def run_batch(qcb):
     b = qcb.Batch(Ls, betas, list(range(len(Ls))))
     b.hot_start()
     variant, tune_ms = b.tune(1, 2, allow_store_change=True)
+    k_tune = b.info()["sweep"]  # the tuning sweeps ran in the 18-real storage
     b.sweep(1, 2)
     b.sync()
     s = torch.cuda.ExternalStream(b.stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    n_sw = 20
     e0.record(s)
-    b.sweep(1, n_sw)
+    b.sweep(1, n_sweeps)
     e1.record(s)
     e1.synchronize()
-    ms = e0.elapsed_time(e1) / n_sw
+    ms = e0.elapsed_time(e1) / n_sweeps
     info = b.info()
+    plaq = b.plaquette()
+    # per-chain check: the chain of each size against its own single-lattice run (same seed and
+    # sweeps; 18-real storage for the tuning sweeps, then the storage the tuner chose)
+    checked, dp = [], 0.0
+    for i in (0, 96, 192, 240):
+        f = qcb.GaugeField(Ls[i], qcb.PREC_F64, qcb.STORE_18)
+        f.hot_start(i)
+        for k in range(info["sweep"]):
+            if k == k_tune and info["store"] != qcb.STORE_18:
+                g = qcb.GaugeField(Ls[i], qcb.PREC_F64, info["store"])
+                g.copy_from(f)
+                f.close()
+                f = g
+            f.hb_sweep(float(betas[i]), 1, i, k)
+        p1 = f.plaquette()
+        f.close()
+        checked.append(i)
+        dp = max(dp, abs(p1 - float(plaq[i])))
     b.close()
     V = sum(L[0] ** 4 for L in Ls)
     serial = 0.0
@@ -380,17 +401,55 @@ def run_batch(qcb):
         per[f"{Lc[0]}^4"] = one
         serial += cnt * one
         f.close()
-    return {"chains": len(Ls), "sites": V, "n_hits": 1, "ms_per_sweep": ms, "link_upd_per_s": 4 * V / (ms * 1e-3),
+    return {"chains": len(Ls), "sites": V, "n_hits": 1, "timed_sweeps": n_sweeps, "total_sweeps": info["sweep"],
+            "ms_per_sweep": ms, "link_upd_per_s": 4 * V / (ms * 1e-3),
             "serial_ms_per_sweep": serial, "serial_single_sweep_ms": per, "speedup_vs_serial": serial / ms,
             "tuned": {"variant": variant, "store": "12" if info["store"] == 1 else "18", "ms": tune_ms},
-            "launches_per_sweep": 9, "graph": True}
+            "launches_per_sweep": 9, "graph": True,
+            "per_chain_check": {"chains": checked, "max_abs_dP_vs_single_chain": dp}}
 
 
-def run_serve(qcb, n_req: int, store: int = 1):
-    """Serving: Poisson arrivals at 100 req/s, L in {8,12,16,20,24,32} with p = (.3,.25,.2,.1,.1,.05),
-    beta ~ U[5.8, 6.3], inputs = 50 FP64 sweeps from seed = request id (excluded from latency), flow
-    eps = 0.02 to t = L^2/32 in FP32 links (12-real storage by default) with FP64 reprojection and
-    Q/E every step; against one-at-a-time plain FP64 flow."""
+def serve_once(qcb, reqs, rate: float, store: int):
+    """One server run: requests (L, input links, steps) submitted at Poisson arrival times of the
+    given rate; returns latency (submit -> result), queue wait (submit -> admission) and rates."""
+    import numpy as np
+
+    arr = np.cumsum(np.random.default_rng(7).exponential(1.0 / rate, len(reqs)))
+    site_steps = sum(int(L) ** 4 * (n - 1) for L, _, n in reqs)
+    srv = qcb.Server(150 << 30, prec=qcb.PREC_F32, store=store)
+    time.sleep(FLOW_COOL_S)  # every arm starts from an idle GPU
+    start = srv.now()
+    k, done = 0, {}
+    while len(done) < len(reqs):
+        now = srv.now() - start
+        while k < len(reqs) and arr[k] <= now:
+            L, U, n = reqs[k]
+            srv.submit(k, (int(L),) * 4, U, 0.02, n)
+            k += 1
+        r = srv.poll()
+        if r is None:
+            time.sleep(0.0005)
+            continue
+        done[r[0]] = r
+    lat = np.array([done[i][2][2] - (start + arr[i]) for i in range(len(reqs))])
+    wait = np.array([done[i][2][1] - done[i][2][0] for i in range(len(reqs))])
+    wall = max(done[i][2][2] for i in range(len(reqs))) - start
+    st = srv.stats()
+    srv.close()
+    return {"rate_per_s": rate, "requests": len(reqs), "offered_site_steps_per_s": site_steps * rate / len(reqs),
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "queue_wait_p50_s": float(np.percentile(wait, 50)), "queue_wait_p99_s": float(np.percentile(wait, 99)),
+            "configs_per_s": len(reqs) / wall, "site_steps_per_s": site_steps / wall,
+            "peak_resident": st["peak_resident"], "peak_bytes": st["peak_bytes"]}
+
+
+def run_serve(qcb, n_req: int, store: int = 1, low_rates=(4.0, 2.0), n_low: int = 12):
+    """Serving (the serving configuration): Poisson arrivals at 100 req/s, L in {8,12,16,20,24,32}
+    with p = (.3,.25,.2,.1,.1,.05), beta ~ U[5.8, 6.3], inputs = 50 FP64 sweeps from seed = request
+    id (excluded from latency), flow eps = 0.02 to t = L^2/32 in FP32 links (12-real storage by
+    default) with FP64 reprojection and Q/E every step; against one-at-a-time plain FP64 flow.
+    100 req/s offers several times what one GPU can flow, so that run measures a saturated queue;
+    the first n_low requests are also offered at the lower rates, below saturation."""
     import numpy as np
 
     rng = np.random.default_rng(2026)
@@ -403,6 +462,7 @@ def run_serve(qcb, n_req: int, store: int = 1):
     inputs = [b.download(i) for i in range(n_req)]
     b.close()
     steps = [int(round(x * x / 32 / 0.02)) + 1 for x in sizes]
+    reqs = list(zip(sizes, inputs, steps))
     site_steps = sum(int(x) ** 4 * (n - 1) for x, n in zip(sizes, steps))
     srv = qcb.Server(150 << 30, prec=qcb.PREC_F32, store=store)
     time.sleep(FLOW_COOL_S)  # both arms start from an idle GPU
@@ -419,6 +479,7 @@ def run_serve(qcb, n_req: int, store: int = 1):
             continue
         done[r[0]] = r
     lat = np.array([done[i][2][2] - (start + arr[i]) for i in range(n_req)])
+    wait = np.array([done[i][2][1] - done[i][2][0] for i in range(n_req)])
     wall = max(done[i][2][2] for i in range(n_req)) - start
     st = srv.stats()
     srv.close()
@@ -437,14 +498,18 @@ def run_serve(qcb, n_req: int, store: int = 1):
         fl.close()
         f.close()
     lat2 = np.array(lat2)
+    low = [serve_once(qcb, reqs[:n_low], r, store) for r in low_rates]
     return {"requests": n_req, "rate_per_s": 100.0, "site_steps": site_steps,
+            "offered_site_steps_per_s": site_steps * 100.0 / n_req, "saturated": True,
             "prec": "fp32-12" if store == 1 else "fp32-18",
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "queue_wait_p50_s": float(np.percentile(wait, 50)), "queue_wait_p99_s": float(np.percentile(wait, 99)),
             "configs_per_s": n_req / wall, "site_steps_per_s": site_steps / wall,
             "peak_resident": st["peak_resident"], "peak_bytes": st["peak_bytes"],
             "serial_fp64": {"p50_s": float(np.percentile(lat2, 50)), "p99_s": float(np.percentile(lat2, 99)),
                             "configs_per_s": n_req / tq, "site_steps_per_s": site_steps / busy},
-            "speedup_configs_per_s": (n_req / wall) / (n_req / tq)}
+            "speedup_configs_per_s": (n_req / wall) / (n_req / tq),
+            "below_saturation": low}
 
 
 def run_ours(args, rank: int, world: int, local: int):
@@ -578,6 +643,7 @@ def run_ours(args, rank: int, world: int, local: int):
             "e2e": {"value": e2e_value, "unit": "link-upd/s", "h2d_bytes_per_step": V * 576,
                     "d2h_bytes_per_step": 8, "steps": n_e2e,
                     "step": "upload FP64 AoS config from pinned host + sweep + plaquette readback via the C ABI"},
+            "hits_per_s": value * N_HITS,
             "gpu_launches": n_launch,
             "clocks": clk.summary(),
             "plaquette_after": plaq,

@@ -123,9 +123,11 @@ int check_err_flag(qcb_field_s* f) {
     int h = 0;
     CK(cudaMemcpyAsync(&h, f->d_err, sizeof(int), cudaMemcpyDeviceToHost, f->stream));
     CK(cudaStreamSynchronize(f->stream));
-    if (h & DERR_KP_CAP) {
+    if (h) {
         CK(cudaMemsetAsync(f->d_err, 0, sizeof(int), f->stream));
-        return fail(QCB_ERANGE, "heatbath: Kennedy-Pendleton attempt cap reached");
+        if (h & DERR_KP_SCALE)
+            return fail(QCB_ERANGE, "heatbath: zero or non-finite SU(2) projection of the staple (link left unchanged)");
+        return fail(QCB_ERANGE, "heatbath: Kennedy-Pendleton attempt cap (2^20) reached (link left unchanged)");
     }
     return QCB_OK;
 }
@@ -187,7 +189,7 @@ WorkList single_list(qcb_field_s* f) {
 int flow_step(qcb_flow_s* fl) {
     qcb_field_s* f = fl->fld;
     RET(ensure_alt(f));
-    const int rep = (f->prec == QCB_PREC_F32) ? 1 : 0;
+    const int rep = needs_reproject(f->prec, f->store);
     for (int stage = 1; stage <= 3; stage++) {
         void* win = (stage == 2) ? f->alt : f->links;
         void* wout = (stage == 2) ? f->links : f->alt;
@@ -500,7 +502,7 @@ int qcb_hb_subsweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_
     if (!f) return fail(QCB_EINVAL, "null field");
     if (parity < 0 || parity > 1 || mu < 0 || mu > 3 || n_hits < 0 || !(beta > 0.0))
         return fail(QCB_EINVAL, "heatbath: parity in {0,1}, mu in 0..3, n_hits >= 0, beta > 0");
-    const int rep = (f->prec == QCB_PREC_F32) ? 1 : 0;
+    const int rep = needs_reproject(f->prec, f->store);
     return launch(f, QCB_K_HB, [&] {
         return fmt_ops(f->fmt).hb1(f->g, f->links, parity, mu, -0.75 / beta, n_hits, seed, sweep, rep, f->d_err,
                                    f->stream);

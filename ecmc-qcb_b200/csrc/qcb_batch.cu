@@ -100,7 +100,7 @@ int layout(qcb_batch_s* b, int fmt) {
 
 int run_phase_set(qcb_batch_s* b, int n_hits, int variant) {
     const WorkList w = batch_list(b);
-    const int rep = (b->prec == QCB_PREC_F32) ? 1 : 0;
+    const int rep = needs_reproject(b->prec, b->store);
     for (int p = 0; p < 2; p++)
         for (int mu = 0; mu < 4; mu++) {
             cudaError_t e = fmt_ops(b->fmt).hb(w, variant, p, mu, n_hits, b->d_sweep, 0u, rep, b->d_err, b->stream);
@@ -163,7 +163,9 @@ int read_err(qcb_batch_s* b) {
     CK(cudaStreamSynchronize(b->stream));
     if (h) {
         CK(cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream));
-        return fail(QCB_ERANGE, "batch heatbath: Kennedy-Pendleton attempt cap reached");
+        if (h & DERR_KP_SCALE)
+            return fail(QCB_ERANGE, "batch heatbath: zero or non-finite SU(2) projection of a staple");
+        return fail(QCB_ERANGE, "batch heatbath: Kennedy-Pendleton attempt cap (2^20) reached");
     }
     return QCB_OK;
 }

@@ -32,6 +32,12 @@ struct TimedLaunch {
 
 }  // namespace qcb
 
+// FP64 reprojection after every link update: always for FP32 links, and for 12-real storage in
+// either precision, whose rebuilt third row conj(r0 x r1) makes an SU(3) matrix only from
+// orthonormal rows; without it the norm errors of the stored rows grow under the updates (an FP64
+// 12-real heatbath chain diverged after ~180 sweeps).
+inline int needs_reproject(int prec, int store) { return (prec == QCB_PREC_F32 || store == QCB_STORE_12) ? 1 : 0; }
+
 struct qcb_field_s {
     int L[4];
     qcb::Geom g;

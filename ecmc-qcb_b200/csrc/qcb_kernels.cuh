@@ -12,7 +12,7 @@ namespace qcb {
 constexpr double kPi = 3.14159265358979323846;
 
 // Device error flags (bit mask written by kernels, read by the host after a sync).
-enum : int { DERR_KP_CAP = 1 };
+enum : int { DERR_KP_CAP = 1, DERR_KP_SCALE = 2 };
 
 // byte reversal of a double (ILDG files are big-endian, src/io/ildg.cpp:25-32)
 __device__ __forceinline__ double bswap_f64(double x) {
@@ -261,12 +261,15 @@ __device__ __forceinline__ KPDraws kp_draws_at(const LinkStream& rng, uint32_t n
 // reference's order: (delta, r1, r2, r3) per Kennedy-Pendleton attempt, then (u_phi, u_cos).
 // With c_alpha = -0.75/beta, -0.5/alpha = c_alpha / k (alpha = 2 beta k / 3), so one rsqrt
 // gives both v = w/k and the attempt scale.
-// The loop is capped at KP_MAX_ATTEMPTS attempts and a non-finite or non-negative scale is
-// rejected up front; in either case the subgroup element is the identity (the link is left
-// unchanged by this subgroup) and the kernel raises DERR_KP_CAP.
+// The reference loops until acceptance.  Here the loop is capped at KP_MAX_ATTEMPTS = 2^20
+// attempts, so that no lane can spin without bound: acceptance falls roughly like alpha^1.5, and
+// the cap is reached only for alpha ~ 1e-4 (|w| ~ 1e-5), which the updates of hot and thermalised
+// configurations never produce.  On the cap the subgroup element is the identity (the link is left
+// unchanged by this subgroup) and the kernel raises DERR_KP_CAP; a zero or non-finite |w| (a
+// non-finite or non-negative scale) is rejected up front in the same way and raises DERR_KP_SCALE.
 // `d` holds this subgroup's first draws on entry; with `more` set it holds the next subgroup's
 // on return (evaluated right after acceptance, alongside the rest of this update).
-constexpr int KP_MAX_ATTEMPTS = 4096;
+constexpr int KP_MAX_ATTEMPTS = 1 << 20;
 __device__ __forceinline__ Quat su2_step(double c_alpha, Quat w, const LinkStream& rng, KPDraws& d, bool more,
                                          int* err) {
     const double ik = rsqrt(w.a0 * w.a0 + w.a1 * w.a1 + w.a2 * w.a2 + w.a3 * w.a3);  // 1/k
@@ -296,7 +299,7 @@ __device__ __forceinline__ Quat su2_step(double c_alpha, Quat w, const LinkStrea
     const uint32_t n_next = ok ? n + 2u * (uint32_t)it + 3u : n + 2u * (uint32_t)cap;
     if (more) d = kp_draws_at(rng, n_next);
     if (!ok) {
-        atomicOr(err, (int)DERR_KP_CAP);
+        atomicOr(err, cap > 0 ? (int)DERR_KP_CAP : (int)DERR_KP_SCALE);
         return Quat{1.0, 0.0, 0.0, 0.0};
     }
     const double rs = sqrt(1.0 - a0 * a0);

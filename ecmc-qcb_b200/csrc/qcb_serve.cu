@@ -264,7 +264,7 @@ bool flow_big(qcb_server_s* s, Request* r, int stage, int flip_xor, int rep) {
 
 void scheduler(qcb_server_s* s) {
     cudaSetDevice(s->device);
-    const int rep = (s->prec == QCB_PREC_F32) ? 1 : 0;
+    const int rep = needs_reproject(s->prec, s->store);
     while (true) {
         std::vector<Request*> fresh;
         {
