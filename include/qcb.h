@@ -37,7 +37,8 @@ extern "C" {
 #define QCB_PREC_F64 64
 #define QCB_PREC_F32 32
 #define QCB_STORE_18 0 /* full 3x3 complex matrix (18 reals) */
-#define QCB_STORE_12 1 /* first two rows (12 reals), third rebuilt in registers */
+#define QCB_STORE_12 1 /* first two rows (12 reals), third rebuilt in registers; links in this
+                          * storage are reprojected to SU(3) in FP64 after every update */
 
 typedef struct qcb_field_s* qcb_field;
 typedef struct qcb_flow_s* qcb_flow;
@@ -99,8 +100,8 @@ int qcb_random_shift(qcb_field f, uint64_t seed, uint64_t idx, int max_shift, in
  * Philox stream keyed on seed and countered on (draw, link, sweep). */
 int qcb_hb_subsweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_t sweep, int parity, int mu);
 /* Full sweep: (parity 0, mu 0..3) then (parity 1, mu 0..3).  Replaces the pair
- * sweep(EV); sweep(OD) of mpi::heatbathcb::samples (heatbath_mpi.cpp:60-75).  FP32 fields
- * are reprojected to SU(3) in FP64 after each sweep. */
+ * sweep(EV); sweep(OD) of mpi::heatbathcb::samples (heatbath_mpi.cpp:60-75).  FP32 fields and
+ * 12-real fields are reprojected to SU(3) in FP64 after each link update. */
 int qcb_hb_sweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_t sweep);
 
 /* ------------------------------------------------------------------ observables */
