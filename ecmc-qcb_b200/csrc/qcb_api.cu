@@ -170,20 +170,6 @@ int download_to_staging(qcb_field_s* f, int bswap) {
                   [&] { return fmt_ops(f->fmt).soa_to_aos(f->g, f->links, f->staging, bswap, f->stream); });
 }
 
-// Work list of a single field (descriptor passed by value).
-WorkList single_list(qcb_field_s* f) {
-    WorkList w;
-    w.one.g = f->g;
-    w.one.links = f->links;
-    w.one.links_out = f->alt;
-    w.one.nb_begin = 0;
-    w.one.nb = (int)((f->g.Vh + TILE - 1) / TILE);
-    w.one.flip = 0;
-    w.nb_total = w.one.nb;
-    w.nlat = 1;
-    return w;
-}
-
 // One RK3 step on the flow's field: stage 1 reads links and writes alt, stage 2 the reverse,
 // stage 3 links -> alt again; the buffers then swap so that links holds the result.
 int flow_step(qcb_flow_s* fl) {
