@@ -92,16 +92,16 @@ struct FmtImpl {
     }
     static cudaError_t flow1(const Geom& g, const void* win, void* wout, void* z, double eps, int stage, int rep,
                              cudaStream_t s) {
-        const unsigned nb = 8u * (unsigned)((g.Vh + QCB_FLOW_THREADS - 1) / QCB_FLOW_THREADS);
+        const unsigned nb = 8u * (unsigned)((g.Vh + QCB_FLOW1_THREADS - 1) / QCB_FLOW1_THREADS);
         AlgField<R> za;
         za.p = (typename AlgField<R>::C2*)z;
         za.Vh = g.Vh;
         if (stage == 1)
-            k_flow_stage<R, NE, 1><<<nb, QCB_FLOW_THREADS, 0, s>>>(g, view(win, g.Vh), view(wout, g.Vh), za, eps, rep);
+            k_flow_stage<R, NE, 1><<<nb, QCB_FLOW1_THREADS, 0, s>>>(g, view(win, g.Vh), view(wout, g.Vh), za, eps, rep);
         else if (stage == 2)
-            k_flow_stage<R, NE, 2><<<nb, QCB_FLOW_THREADS, 0, s>>>(g, view(win, g.Vh), view(wout, g.Vh), za, eps, rep);
+            k_flow_stage<R, NE, 2><<<nb, QCB_FLOW1_THREADS, 0, s>>>(g, view(win, g.Vh), view(wout, g.Vh), za, eps, rep);
         else
-            k_flow_stage<R, NE, 3><<<nb, QCB_FLOW_THREADS, 0, s>>>(g, view(win, g.Vh), view(wout, g.Vh), za, eps, rep);
+            k_flow_stage<R, NE, 3><<<nb, QCB_FLOW1_THREADS, 0, s>>>(g, view(win, g.Vh), view(wout, g.Vh), za, eps, rep);
         return cudaGetLastError();
     }
 

@@ -230,6 +230,13 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
 #ifndef QCB_CLOVER_MINB
 #define QCB_CLOVER_MINB(R) (sizeof(R) == 8 ? 2 : 4)
 #endif
+// single-lattice flow stage launch shape (the tiled kernels keep QCB_FLOW_THREADS = TILE)
+#ifndef QCB_FLOW1_THREADS
+#define QCB_FLOW1_THREADS QCB_FLOW_THREADS
+#endif
+#ifndef QCB_FLOW1_MINB
+#define QCB_FLOW1_MINB(R) QCB_FLOW_MINB(R)
+#endif
 #ifndef QCB_FLOW_RTMU
 #define QCB_FLOW_RTMU 1
 #endif
@@ -639,7 +646,7 @@ __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>&
 // Single-lattice RK3 stage.  Grid: blockIdx.x = (site block) * 8 + (mu*2 + parity), so the 8
 // link classes of a block of sites run together and share their neighbour links in L2.
 template <typename R, int NE, int STAGE>
-__global__ void __launch_bounds__(QCB_FLOW_THREADS, QCB_FLOW_MINB(R))
+__global__ void __launch_bounds__(QCB_FLOW1_THREADS, QCB_FLOW1_MINB(R))
     k_flow_stage(Geom g, LinkField<R, NE> Win, LinkField<R, NE> Wout, AlgField<R> Z, double eps, int reproject) {
     const int lt = blockIdx.x & 7;
     const int64_t h = (int64_t)(blockIdx.x >> 3) * blockDim.x + threadIdx.x;
