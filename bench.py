@@ -523,6 +523,26 @@ def run_ours(args, rank: int, world: int, local: int):
     f.hot_start(SEED_HOT)
     stream, e0, e1 = cuda_timer(qcb, f)
 
+    if args.only == "obs":
+        # observables and 12-real heatbath of every form on the configuration (for ncu captures):
+        # per form `steps` plaquette and clover passes; then 2 FP64 12-real heatbath sweeps
+        for i in range(args.warmup):
+            f.hb_sweep(BETA, N_HITS, SEED_HB, i)
+        for prec, store in ((64, 0), (64, 1), (32, 0), (32, 1)):
+            g = qcb.GaugeField(L, prec, store)
+            g.copy_from(f)
+            for k in range(args.steps):
+                g.plaquette()
+                g.clover_qe()
+            g.close()
+        g = qcb.GaugeField(L, qcb.PREC_F64, qcb.STORE_12)
+        g.copy_from(f)
+        for k in range(2):
+            g.hb_sweep(BETA, N_HITS, SEED_HB, 1000 + k)
+        g.close()
+        f.close()
+        return
+
     if args.only == "flow":
         for i in range(args.warmup):
             f.hb_sweep(BETA, N_HITS, SEED_HB, i)
@@ -665,7 +685,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="length of the CPU-baseline sample (0 skips it)")
-    ap.add_argument("--only", default="all", choices=["all", "hb", "flow"],
+    ap.add_argument("--only", default="all", choices=["all", "hb", "flow", "obs"],
                     help="run one part (used for ncu captures of a single kernel family)")
     ap.add_argument("--parts", default="all", choices=["all", "core"],
                     help="core: skip the batch and serving sections")

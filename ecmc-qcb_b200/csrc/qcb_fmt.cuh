@@ -118,11 +118,11 @@ struct FmtImpl {
     }
 
     static cudaError_t plaquette(const Geom& g, const void* links, double* partials, unsigned nbx, cudaStream_t s) {
-        k_plaquette<R, NE><<<dim3(nbx, 2), 256, 0, s>>>(g, view(links, g.Vh), partials);
+        k_plaquette<R, NE><<<dim3(2, nbx), 256, 0, s>>>(g, view(links, g.Vh), partials);
         return cudaGetLastError();
     }
     static cudaError_t clover(const Geom& g, const void* links, double* partials, unsigned nbx, cudaStream_t s) {
-        k_clover_qe<R, NE><<<dim3(nbx, 6), 128, 0, s>>>(g, view(links, g.Vh), partials);
+        k_clover_qe<R, NE><<<dim3(6, nbx), 128, 0, s>>>(g, view(links, g.Vh), partials);
         return cudaGetLastError();
     }
     static cudaError_t unitarity(const Geom& g, const void* links, double* partials, unsigned nbx, cudaStream_t s) {

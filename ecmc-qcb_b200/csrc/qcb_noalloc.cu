@@ -94,7 +94,7 @@ extern "C" int qcb_plaquette_noalloc(const int L[4], const double* d_links, doub
     LinkField<double, 9, false> U;  // the caller's untiled layout
     U.p = (double2*)d_links;
     U.Vh = g.Vh;
-    k_plaquette<double, 9, false><<<dim3(nbx, 2), 256, 0, s>>>(g, U, (double*)scratch);
+    k_plaquette<double, 9, false><<<dim3(2, nbx), 256, 0, s>>>(g, U, (double*)scratch);
     k_noalloc_final<<<1, 256, 0, s>>>((const double*)scratch, nb, 6.0 * (double)V, d_plaq);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(QCB_ECUDA, "plaquette_noalloc launch: %s", cudaGetErrorString(e));
