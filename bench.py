@@ -443,13 +443,14 @@ def serve_once(qcb, reqs, rate: float, store: int):
             "peak_resident": st["peak_resident"], "peak_bytes": st["peak_bytes"]}
 
 
-def run_serve(qcb, n_req: int, store: int = 1, low_rates=(4.0, 2.0), n_low: int = 12):
+def run_serve(qcb, n_req: int, stores=(0, 1), low_rates=(4.0, 2.0), n_low: int = 12):
     """Serving (the serving configuration): Poisson arrivals at 100 req/s, L in {8,12,16,20,24,32}
     with p = (.3,.25,.2,.1,.1,.05), beta ~ U[5.8, 6.3], inputs = 50 FP64 sweeps from seed = request
-    id (excluded from latency), flow eps = 0.02 to t = L^2/32 in FP32 links (12-real storage by
-    default) with FP64 reprojection and Q/E every step; against one-at-a-time plain FP64 flow.
-    100 req/s offers several times what one GPU can flow, so that run measures a saturated queue;
-    the first n_low requests are also offered at the lower rates, below saturation."""
+    id (excluded from latency), flow eps = 0.02 to t = L^2/32 in FP32 links with FP64 reprojection
+    and Q/E every step; against one-at-a-time plain FP64 flow.  The saturated run is made in each
+    FP32 storage of `stores`; the faster is reported at the top level (the other under
+    "other_storage").  100 req/s offers several times what one GPU can flow, so that run measures a
+    saturated queue; the first n_low requests are also offered at the lower rates, below saturation."""
     import numpy as np
 
     rng = np.random.default_rng(2026)
@@ -464,32 +465,42 @@ def run_serve(qcb, n_req: int, store: int = 1, low_rates=(4.0, 2.0), n_low: int 
     steps = [int(round(x * x / 32 / 0.02)) + 1 for x in sizes]
     reqs = list(zip(sizes, inputs, steps))
     site_steps = sum(int(x) ** 4 * (n - 1) for x, n in zip(sizes, steps))
-    srv = qcb.Server(150 << 30, prec=qcb.PREC_F32, store=store)
-    time.sleep(FLOW_COOL_S)  # both arms start from an idle GPU
-    start = srv.now()
-    k, done = 0, {}
-    while len(done) < n_req:
-        now = srv.now() - start
-        while k < n_req and arr[k] <= now:
-            srv.submit(k, (int(sizes[k]),) * 4, inputs[k], 0.02, steps[k])
-            k += 1
-        r = srv.poll()
-        if r is None:
-            time.sleep(0.0005)
-            continue
-        done[r[0]] = r
-    lat = np.array([done[i][2][2] - (start + arr[i]) for i in range(n_req)])
-    wait = np.array([done[i][2][1] - done[i][2][0] for i in range(n_req)])
-    wall = max(done[i][2][2] for i in range(n_req)) - start
-    st = srv.stats()
-    srv.close()
+    arms = {}
+    for store in stores:
+        srv = qcb.Server(150 << 30, prec=qcb.PREC_F32, store=store)
+        time.sleep(FLOW_COOL_S)  # every arm starts from an idle GPU
+        start = srv.now()
+        k, done = 0, {}
+        while len(done) < n_req:
+            now = srv.now() - start
+            while k < n_req and arr[k] <= now:
+                srv.submit(k, (int(sizes[k]),) * 4, inputs[k], 0.02, steps[k])
+                k += 1
+            r = srv.poll()
+            if r is None:
+                time.sleep(0.0005)
+                continue
+            done[r[0]] = r
+        lat = np.array([done[i][2][2] - (start + arr[i]) for i in range(n_req)])
+        wait = np.array([done[i][2][1] - done[i][2][0] for i in range(n_req)])
+        wall = max(done[i][2][2] for i in range(n_req)) - start
+        st = srv.stats()
+        srv.close()
+        arms[store] = {"prec": "fp32-12" if store == 1 else "fp32-18",
+                       "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                       "queue_wait_p50_s": float(np.percentile(wait, 50)),
+                       "queue_wait_p99_s": float(np.percentile(wait, 99)),
+                       "configs_per_s": n_req / wall, "site_steps_per_s": site_steps / wall,
+                       "peak_resident": st["peak_resident"], "peak_bytes": st["peak_bytes"]}
+    store = max(arms, key=lambda s_: arms[s_]["configs_per_s"])
     tq, lat2, busy = 0.0, [], 0.0
     time.sleep(FLOW_COOL_S)
     for i in range(n_req):
+        # one request at a time, from its host configuration to its results, as the server takes it
+        t0 = time.perf_counter()
         f = qcb.GaugeField((int(sizes[i]),) * 4, 64, 0)
         f.upload(inputs[i])
         fl = qcb.GradientFlow(f, 0.02, prec=64, store=0)
-        t0 = time.perf_counter()
         fl.measure(f, steps[i], 1)
         dt = time.perf_counter() - t0
         busy += dt
@@ -499,17 +510,18 @@ def run_serve(qcb, n_req: int, store: int = 1, low_rates=(4.0, 2.0), n_low: int 
         f.close()
     lat2 = np.array(lat2)
     low = [serve_once(qcb, reqs[:n_low], r, store) for r in low_rates]
-    return {"requests": n_req, "rate_per_s": 100.0, "site_steps": site_steps,
-            "offered_site_steps_per_s": site_steps * 100.0 / n_req, "saturated": True,
-            "prec": "fp32-12" if store == 1 else "fp32-18",
-            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-            "queue_wait_p50_s": float(np.percentile(wait, 50)), "queue_wait_p99_s": float(np.percentile(wait, 99)),
-            "configs_per_s": n_req / wall, "site_steps_per_s": site_steps / wall,
-            "peak_resident": st["peak_resident"], "peak_bytes": st["peak_bytes"],
-            "serial_fp64": {"p50_s": float(np.percentile(lat2, 50)), "p99_s": float(np.percentile(lat2, 99)),
-                            "configs_per_s": n_req / tq, "site_steps_per_s": site_steps / busy},
-            "speedup_configs_per_s": (n_req / wall) / (n_req / tq),
-            "below_saturation": low}
+    out = {"requests": n_req, "rate_per_s": 100.0, "site_steps": site_steps,
+           "offered_site_steps_per_s": site_steps * 100.0 / n_req, "saturated": True}
+    out.update(arms[store])
+    out.update({"serial_fp64": {"p50_s": float(np.percentile(lat2, 50)), "p99_s": float(np.percentile(lat2, 99)),
+                                "configs_per_s": n_req / tq, "site_steps_per_s": site_steps / busy},
+                "speedup_configs_per_s": arms[store]["configs_per_s"] / (n_req / tq),
+                "other_storage": {a["prec"]: {"configs_per_s": a["configs_per_s"], "p50_s": a["p50_s"],
+                                              "p99_s": a["p99_s"],
+                                              "speedup_configs_per_s": a["configs_per_s"] / (n_req / tq)}
+                                  for s_, a in arms.items() if s_ != store},
+                "below_saturation": low})
+    return out
 
 
 def run_ours(args, rank: int, world: int, local: int):
