@@ -11,7 +11,8 @@
 //     the tile work list of all of them, so requests that arrive while others are on the GPU
 //     share the same launches; a request of kBigVh half-sites or more fills the GPU by itself and
 //     runs the single-lattice kernels (geometry in kernel parameters, no per-tile descriptor
-//     lookups), in the same stream between the shared launches;
+//     lookups).  Big requests run on one stream and the shared launches of the small ones on a
+//     second, so the small requests' short launches overlap the big requests' kernels;
 //   * a request that has taken its last measurement is copied back, frees its memory and is
 //     handed to qcb_serve_poll with its submit and completion times.
 // Per-request results do not depend on the other requests in the mix: every link and every
@@ -51,6 +52,7 @@ struct Request {
     size_t off_out = 0, off_z = 0, off_meas = 0;
     int tick0 = 0;
     int flip = 0;
+    cudaStream_t st = nullptr;  // the stream of all its work (big or small requests' stream)
 };
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -79,7 +81,10 @@ struct qcb_server_s {
     int err = QCB_OK;
     std::string errmsg;
     std::thread th;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;        // big requests (single-lattice kernels)
+    cudaStream_t stream_small = nullptr;  // small requests (shared tiled launches)
+    cudaEvent_t ev_layout = nullptr;      // last conversion out of the shared upload staging
+    bool layout_pending = false;
     cudaMemPool_t pool = nullptr;
     // work list of the active set
     std::vector<LatDesc> desc;
@@ -186,22 +191,28 @@ bool rebuild(qcb_server_s* s) {
     if (!grow(s, &s->partials, &s->partials_cap, (size_t)12 * nb)) return false;
     // pageable sources: the copies are staged before the calls return
     if (!cuda_ok(s, cudaMemcpyAsync(s->d_desc, s->desc.data(), sizeof(LatDesc) * s->desc.size(),
-                                    cudaMemcpyHostToDevice, s->stream), "descriptor upload"))
+                                    cudaMemcpyHostToDevice, s->stream_small), "descriptor upload"))
         return false;
     return cuda_ok(s, cudaMemcpyAsync(s->d_tile_lat, tile_lat.data(), sizeof(int) * tile_lat.size(),
-                                      cudaMemcpyHostToDevice, s->stream), "tile map upload");
+                                      cudaMemcpyHostToDevice, s->stream_small), "tile map upload");
 }
 
+// Admission on the request's stream; the upload into the shared staging waits until the previous
+// admission's conversion (on either stream) has read it.
 bool admit(qcb_server_s* s, Request* r) {
     r->t_admit = s->now();
-    if (!cuda_ok(s, cudaMallocFromPoolAsync(&r->buf, r->bytes, s->pool, s->stream), "request allocation")) return false;
+    r->st = is_big(r) ? s->stream : s->stream_small;
+    if (!cuda_ok(s, cudaMallocFromPoolAsync(&r->buf, r->bytes, s->pool, r->st), "request allocation")) return false;
     const size_t nd = (size_t)r->g.V * 72;
     if (!grow(s, &s->staging, &s->staging_cap, nd / 2)) return false;
-    if (!cuda_ok(s, cudaMemcpyAsync(s->staging, r->input.data(), nd * sizeof(double), cudaMemcpyHostToDevice, s->stream),
+    if (s->layout_pending && !cuda_ok(s, cudaStreamWaitEvent(r->st, s->ev_layout, 0), "upload order")) return false;
+    if (!cuda_ok(s, cudaMemcpyAsync(s->staging, r->input.data(), nd * sizeof(double), cudaMemcpyHostToDevice, r->st),
                  "request upload"))
         return false;
-    if (!cuda_ok(s, fmt_ops(s->fmt).aos_to_soa(r->g, s->staging, r->buf, 0, s->stream), "request layout")) return false;
+    if (!cuda_ok(s, fmt_ops(s->fmt).aos_to_soa(r->g, s->staging, r->buf, 0, r->st), "request layout")) return false;
     note_launches(1);
+    if (!cuda_ok(s, cudaEventRecord(s->ev_layout, r->st), "layout event")) return false;
+    s->layout_pending = true;
     std::vector<double>().swap(r->input);
     r->tick0 = s->tick;
     r->flip = (int)(s->nflow & 1);  // current links in buffer A
@@ -211,10 +222,10 @@ bool admit(qcb_server_s* s, Request* r) {
 bool finish(qcb_server_s* s, Request* r) {
     std::vector<double> meas((size_t)r->n_steps * 3);
     if (!cuda_ok(s, cudaMemcpyAsync(meas.data(), (char*)r->buf + r->off_meas, meas.size() * sizeof(double),
-                                    cudaMemcpyDeviceToHost, s->stream), "result readback"))
+                                    cudaMemcpyDeviceToHost, r->st), "result readback"))
         return false;
-    if (!cuda_ok(s, cudaFreeAsync(r->buf, s->stream), "request free")) return false;
-    if (!cuda_ok(s, cudaStreamSynchronize(s->stream), "result sync")) return false;
+    if (!cuda_ok(s, cudaFreeAsync(r->buf, r->st), "request free")) return false;
+    if (!cuda_ok(s, cudaStreamSynchronize(r->st), "result sync")) return false;
     r->buf = nullptr;
     r->tqe.resize((size_t)r->n_steps * 3);
     double t = 0.0;
@@ -297,8 +308,9 @@ void scheduler(qcb_server_s* s) {
         w.nlat = (int)s->small.size();
         const int fx = (int)(s->nflow & 1);
         if (!s->small.empty()) {
-            if (!cuda_ok(s, fmt_ops(s->fmt).clover_tiles(w, fx, s->partials, s->stream), "clover launch")) break;
-            k_meas_finalize<<<(unsigned)s->small.size(), 256, 0, s->stream>>>(s->d_desc, s->partials, s->tick);
+            if (!cuda_ok(s, fmt_ops(s->fmt).clover_tiles(w, fx, s->partials, s->stream_small), "clover launch"))
+                break;
+            k_meas_finalize<<<(unsigned)s->small.size(), 256, 0, s->stream_small>>>(s->d_desc, s->partials, s->tick);
             if (!cuda_ok(s, cudaGetLastError(), "measure finalize")) break;
             note_launches(2);
         }
@@ -322,7 +334,7 @@ void scheduler(qcb_server_s* s) {
             const int f = (int)(s->nflow & 1);
             for (int stage = 1; stage <= 3 && ok; stage++) {
                 if (!s->small.empty()) {
-                    ok = cuda_ok(s, fmt_ops(s->fmt).flow(w, stage, f, rep, s->stream), "flow launch");
+                    ok = cuda_ok(s, fmt_ops(s->fmt).flow(w, stage, f, rep, s->stream_small), "flow launch");
                     note_launches(1);
                 }
                 for (Request* r : s->big) ok = ok && flow_big(s, r, stage, f, rep);
@@ -344,6 +356,7 @@ void scheduler(qcb_server_s* s) {
         }
     }
     cudaStreamSynchronize(s->stream);
+    cudaStreamSynchronize(s->stream_small);
 }
 
 }  // namespace
@@ -365,6 +378,8 @@ int qcb_serve_create(size_t hbm_budget_bytes, int prec, int store, int n_rk, int
     s->t0 = std::chrono::steady_clock::now();
     cudaGetDevice(&s->device);
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream_small, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_layout, cudaEventDisableTiming);
     if (e == cudaSuccess) {
         cudaMemPoolProps props;
         memset(&props, 0, sizeof(props));
@@ -396,13 +411,16 @@ int qcb_serve_destroy(qcb_server s) {
     s->cv_work.notify_all();
     if (s->th.joinable()) s->th.join();
     if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->stream_small) cudaStreamSynchronize(s->stream_small);
     for (Request* r : s->active) {
-        if (r->buf) cudaFreeAsync(r->buf, s->stream);
+        if (r->buf) cudaFreeAsync(r->buf, r->st ? r->st : s->stream);
         delete r;
     }
     for (Request* r : s->pending) delete r;
     for (Request* r : s->done) delete r;
     if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->stream_small) cudaStreamSynchronize(s->stream_small);
+    if (s->ev_layout) cudaEventDestroy(s->ev_layout);
     if (s->d_desc) cudaFree(s->d_desc);
     if (s->d_tile_lat) cudaFree(s->d_tile_lat);
     if (s->partials) cudaFree(s->partials);
@@ -410,6 +428,7 @@ int qcb_serve_destroy(qcb_server s) {
     if (s->staging) cudaFree(s->staging);
     if (s->pool) cudaMemPoolDestroy(s->pool);
     if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->stream_small) cudaStreamDestroy(s->stream_small);
     delete s;
     return QCB_OK;
 }
