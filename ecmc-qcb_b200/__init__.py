@@ -21,6 +21,7 @@ LIB_PATH = os.path.join(HERE, "libqcb.so")
 PREC_F64, PREC_F32 = 64, 32
 STORE_18, STORE_12 = 0, 1
 K_HB, K_FLOW, K_PLAQ, K_CLOVER, K_OTHER = range(5)
+ILDG_SCIDAC_CHECKSUM = 1
 
 ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "EIO", -4: "EFORMAT", -5: "ECUDA", -6: "ETIMEOUT", -7: "ERANGE"}
 
@@ -76,6 +77,8 @@ def exported_symbols():
         "qcb_ildg_write": (i, [_vp, C.c_char_p]),
         "qcb_ildg_read": (i, [_vp, C.c_char_p]),
         "qcb_ildg_probe": (i, [C.c_char_p, _i4, pi]),
+        "qcb_ildg_write_ex": (i, [_vp, C.c_char_p, i]),
+        "qcb_scidac_checksum": (i, [_vp, u64, u64, C.POINTER(u32), C.POINTER(u32)]),
         "qcb_timing_enable": (i, [_vp, i]),
         "qcb_timing_read": (i, [_vp, i, C.POINTER(C.c_long), pd]),
         "qcb_timing_reset": (i, [_vp]),
@@ -250,8 +253,11 @@ class GaugeField:
         return out
 
     # -- ILDG
-    def save_ildg(self, path: str) -> None:
-        _check(lib().qcb_ildg_write(self.h, os.fsencode(path)))
+    def save_ildg(self, path: str, scidac_checksum: bool = False) -> None:
+        if scidac_checksum:
+            _check(lib().qcb_ildg_write_ex(self.h, os.fsencode(path), ILDG_SCIDAC_CHECKSUM))
+        else:
+            _check(lib().qcb_ildg_write(self.h, os.fsencode(path)))
 
     def read_ildg(self, path: str) -> None:
         _check(lib().qcb_ildg_read(self.h, os.fsencode(path)))
@@ -398,6 +404,17 @@ def ildg_probe(path: str):
     p = C.c_int()
     _check(lib().qcb_ildg_probe(os.fsencode(path), L, C.byref(p)))
     return tuple(int(v) for v in L), p.value
+
+
+def scidac_checksum(payload, site_bytes: int):
+    """SciDAC (suma, sumb) of a payload laid out as records of site_bytes bytes in rank order."""
+    buf = memoryview(payload).cast("B")
+    if len(buf) % site_bytes:
+        raise ValueError("payload is not a whole number of site records")
+    a, b = C.c_uint32(), C.c_uint32()
+    arr = (C.c_ubyte * len(buf)).from_buffer_copy(buf) if buf.readonly else (C.c_ubyte * len(buf)).from_buffer(buf)
+    _check(lib().qcb_scidac_checksum(arr, len(buf) // site_bytes, site_bytes, C.byref(a), C.byref(b)))
+    return a.value, b.value
 
 
 class GradientFlow:

@@ -13,10 +13,22 @@
 // big-endian FP64 links in site order t,z,y,x (x fastest), mu = x,y,z,t, row-major 3x3.
 // The reader accepts 64- and 32-bit payloads and non-hypercubic extents; it rejects a
 // payload whose size does not match the lattice (ildg.cpp:142-168).
+//
+// SciDAC checksums (the USQCD QIO site checksum; the reference neither writes nor checks them):
+// for the site of lexicographic rank r (the payload's site order) with bytes b_r as stored,
+// c_r = CRC-32(b_r) (the ISO-HDLC / zlib CRC: reflected polynomial 0xEDB88320, initial and final
+// XOR 0xFFFFFFFF), suma = XOR_r rotl(c_r, r mod 29), sumb = XOR_r rotl(c_r, r mod 31).  They
+// travel as a "scidac-checksum" record, <scidacChecksum><version>1.0</version><suma>hex</suma>
+// <sumb>hex</sumb></scidacChecksum>, after the binary record.  The writer adds it on request
+// only, so its default output stays byte-identical to the reference's; the reader checks it
+// whenever a file carries one.
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "qcb_internal.h"
@@ -84,6 +96,91 @@ bool xml_int(const std::string& xml, const char* tag, int* out) {
     return true;
 }
 
+// CRC-32 by slicing-by-8: T[0] is the byte-wise table of the reflected polynomial, and
+// T[k][i] = (T[k-1][i] >> 8) ^ T[0][T[k-1][i] & 0xff] advances a byte's contribution by k more
+// bytes, so eight input bytes fold into the register with eight lookups.
+struct Crc32Tables {
+    uint32_t t[8][256];
+    Crc32Tables() {
+        for (uint32_t i = 0; i < 256; i++) {
+            uint32_t c = i;
+            for (int k = 0; k < 8; k++) c = (c & 1) ? (c >> 1) ^ 0xEDB88320u : c >> 1;
+            t[0][i] = c;
+        }
+        for (int k = 1; k < 8; k++)
+            for (int i = 0; i < 256; i++) t[k][i] = (t[k - 1][i] >> 8) ^ t[0][t[k - 1][i] & 0xff];
+    }
+};
+
+uint32_t crc32(const unsigned char* p, size_t n) {
+    static const Crc32Tables tab;
+    const auto& t = tab.t;
+    uint32_t c = 0xFFFFFFFFu;
+    for (; n >= 8; n -= 8, p += 8) {
+        const uint32_t lo = c ^ ((uint32_t)p[0] | (uint32_t)p[1] << 8 | (uint32_t)p[2] << 16 | (uint32_t)p[3] << 24);
+        c = t[7][lo & 0xff] ^ t[6][(lo >> 8) & 0xff] ^ t[5][(lo >> 16) & 0xff] ^ t[4][lo >> 24] ^ t[3][p[4]] ^
+            t[2][p[5]] ^ t[1][p[6]] ^ t[0][p[7]];
+    }
+    for (; n > 0; n--, p++) c = t[0][(c ^ *p) & 0xff] ^ (c >> 8);
+    return c ^ 0xFFFFFFFFu;
+}
+
+inline uint32_t rotl32(uint32_t v, unsigned r) { return r ? (v << r) | (v >> (32 - r)) : v; }
+
+// SciDAC suma / sumb of n_sites records of site_bytes each; sites split over host threads (the
+// XOR sums do not depend on the order).
+void scidac_sums(const unsigned char* data, uint64_t n_sites, size_t site_bytes, uint32_t* suma, uint32_t* sumb) {
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const uint64_t per = std::max<uint64_t>(4096, (n_sites + hw - 1) / hw);
+    const unsigned nt = (unsigned)std::max<uint64_t>(1, (n_sites + per - 1) / per);
+    std::vector<uint32_t> a(nt, 0), b(nt, 0);
+    auto work = [&](unsigned k) {
+        const uint64_t r0 = k * per, r1 = std::min(n_sites, r0 + per);
+        uint32_t x = 0, y = 0;
+        for (uint64_t r = r0; r < r1; r++) {
+            const uint32_t c = crc32(data + r * site_bytes, site_bytes);
+            x ^= rotl32(c, (unsigned)(r % 29));
+            y ^= rotl32(c, (unsigned)(r % 31));
+        }
+        a[k] = x;
+        b[k] = y;
+    };
+    std::vector<std::thread> th;
+    for (unsigned k = 1; k < nt; k++) th.emplace_back(work, k);
+    work(0);
+    for (auto& t : th) t.join();
+    uint32_t x = 0, y = 0;
+    for (unsigned k = 0; k < nt; k++) {
+        x ^= a[k];
+        y ^= b[k];
+    }
+    *suma = x;
+    *sumb = y;
+}
+
+std::string scidac_xml(uint32_t suma, uint32_t sumb) {
+    char buf[256];
+    snprintf(buf, sizeof(buf),
+             "<?xml version=\"1.0\" encoding=\"UTF-8\"?><scidacChecksum><version>1.0</version>"
+             "<suma>%x</suma><sumb>%x</sumb></scidacChecksum>",
+             suma, sumb);
+    return buf;
+}
+
+// Hex value of <tag>...</tag>; false when absent or not hexadecimal.
+bool xml_hex(const std::string& xml, const char* tag, uint32_t* v) {
+    const std::string open = std::string("<") + tag + ">";
+    size_t a = xml.find(open);
+    if (a == std::string::npos) return false;
+    a += open.size();
+    while (a < xml.size() && isspace((unsigned char)xml[a])) a++;
+    char* end = nullptr;
+    const unsigned long x = strtoul(xml.c_str() + a, &end, 16);
+    if (end == xml.c_str() + a || x > 0xFFFFFFFFul) return false;
+    *v = (uint32_t)x;
+    return true;
+}
+
 struct LimeScan {
     bool have_xml = false;
     int L[4] = {0, 0, 0, 0};
@@ -91,6 +188,8 @@ struct LimeScan {
     bool have_bin = false;
     long bin_offset = 0;
     uint64_t bin_len = 0;
+    bool have_sum = false;
+    uint32_t suma = 0, sumb = 0;
 };
 
 // Walks the LIME records of the file, reading the "ildg-format" XML and locating the
@@ -120,6 +219,12 @@ int scan(FILE* fp, LimeScan* s) {
             ok &= xml_int(xml, "lt", &s->L[3]);
             if (!xml_int(xml, "precision", &s->precision)) s->precision = 0;
             s->have_xml = ok != 0;
+        } else if (strcmp(type, "scidac-checksum") == 0 && len < (1u << 16) && !s->have_sum) {
+            std::string xml((size_t)len, '\0');
+            if (fread(&xml[0], 1, (size_t)len, fp) != len) return fail(QCB_EFORMAT, "truncated scidac-checksum record");
+            if (!xml_hex(xml, "suma", &s->suma) || !xml_hex(xml, "sumb", &s->sumb))
+                return fail(QCB_EFORMAT, "scidac-checksum record without hexadecimal suma/sumb");
+            s->have_sum = true;
         } else if (strcmp(type, "ildg-binary-data") == 0 && !s->have_bin) {
             s->have_bin = true;
             s->bin_offset = data;
@@ -137,8 +242,18 @@ int scan(FILE* fp, LimeScan* s) {
 
 extern "C" {
 
-int qcb_ildg_write(qcb_field f, const char* path) {
+int qcb_scidac_checksum(const void* payload, uint64_t n_sites, uint64_t site_bytes, uint32_t* suma, uint32_t* sumb) {
+    if ((!payload && n_sites > 0) || !suma || !sumb || site_bytes == 0) return fail(QCB_EINVAL, "null argument");
+    scidac_sums((const unsigned char*)payload, n_sites, (size_t)site_bytes, suma, sumb);
+    return QCB_OK;
+}
+
+int qcb_ildg_write(qcb_field f, const char* path) { return qcb_ildg_write_ex(f, path, 0); }
+
+int qcb_ildg_write_ex(qcb_field f, const char* path, int flags) {
     if (!f || !path) return fail(QCB_EINVAL, "null argument");
+    if (flags & ~QCB_ILDG_SCIDAC_CHECKSUM) return fail(QCB_EINVAL, "unknown ILDG write flags 0x%x", flags);
+    const bool with_sum = (flags & QCB_ILDG_SCIDAC_CHECKSUM) != 0;
     const size_t nd = (size_t)f->g.V * 72;
     std::vector<double> buf(nd);
     int r = field_download_host(f, buf.data(), 1);
@@ -151,8 +266,18 @@ int qcb_ildg_write(qcb_field f, const char* path) {
     static const char zeros[8] = {0};
     size_t pad = (8 - xml.size() % 8) % 8;
     ok = ok && fwrite(zeros, 1, pad, fp) == pad;
-    ok = ok && write_header(fp, "ildg-binary-data", (uint64_t)nd * 8, false, true);
+    // with a checksum the binary record no longer ends the message: the checksum record does
+    ok = ok && write_header(fp, "ildg-binary-data", (uint64_t)nd * 8, false, !with_sum);
     ok = ok && fwrite(buf.data(), 8, nd, fp) == nd;
+    if (with_sum) {
+        uint32_t a = 0, b = 0;
+        scidac_sums((const unsigned char*)buf.data(), (uint64_t)f->g.V, 72 * 8, &a, &b);
+        const std::string sx = scidac_xml(a, b);
+        ok = ok && write_header(fp, "scidac-checksum", sx.size(), false, true);
+        ok = ok && fwrite(sx.data(), 1, sx.size(), fp) == sx.size();
+        const size_t spad = (8 - sx.size() % 8) % 8;
+        ok = ok && fwrite(zeros, 1, spad, fp) == spad;
+    }
     ok = (fclose(fp) == 0) && ok;
     if (!ok) return fail(QCB_EIO, "write failed: %s", path);
     return QCB_OK;
@@ -204,11 +329,14 @@ int qcb_ildg_read(qcb_field f, const char* path) {
     }
     std::vector<double> buf(n);
     bool ok = fseek(fp, s.bin_offset, SEEK_SET) == 0;
+    uint32_t a = 0, b = 0;
     if (ok && prec == 64) {
         ok = fread(buf.data(), 8, n, fp) == n;
+        if (ok && s.have_sum) scidac_sums((const unsigned char*)buf.data(), (uint64_t)f->g.V, 72 * 8, &a, &b);
     } else if (ok) {
         std::vector<uint32_t> b32(n);
         ok = fread(b32.data(), 4, n, fp) == n;
+        if (ok && s.have_sum) scidac_sums((const unsigned char*)b32.data(), (uint64_t)f->g.V, 72 * 4, &a, &b);
         for (uint64_t i = 0; ok && i < n; i++) {
             uint32_t v = __builtin_bswap32(b32[i]);
             float x;
@@ -218,6 +346,8 @@ int qcb_ildg_read(qcb_field f, const char* path) {
     }
     fclose(fp);
     if (!ok) return fail(QCB_EFORMAT, "truncated binary payload in %s", path);
+    if (s.have_sum && (a != s.suma || b != s.sumb))
+        return fail(QCB_EFORMAT, "SciDAC checksum mismatch in %s: file %x %x, payload %x %x", path, s.suma, s.sumb, a, b);
     return field_upload_host(f, buf.data(), prec == 64 ? 1 : 0);
 }
 

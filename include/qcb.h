@@ -131,12 +131,21 @@ qcb_field qcb_flow_field(qcb_flow fl);
 /* save_ildg_clime (src/io/ildg.cpp:34-136): LIME records "ildg-format" (MB=1, ME=1) and
  * "ildg-binary-data" (MB=0, ME=1), big-endian FP64, site order t,z,y,x, mu = x,y,z,t. */
 int qcb_ildg_write(qcb_field f, const char* path);
+/* qcb_ildg_write with flags.  QCB_ILDG_SCIDAC_CHECKSUM appends a "scidac-checksum" record
+ * (MB=0, ME=1; the binary record then has ME=0) holding the SciDAC suma/sumb of the payload. */
+#define QCB_ILDG_SCIDAC_CHECKSUM 1
+int qcb_ildg_write_ex(qcb_field f, const char* path, int flags);
 /* read_ildg_clime (src/io/ildg.cpp:138-237): finds "ildg-binary-data", checks its size
  * against the lattice, reads 64- or 32-bit payloads (precision from the "ildg-format"
- * record when present). */
+ * record when present).  A "scidac-checksum" record, when the file has one, is checked
+ * against the payload (QCB_EFORMAT on a mismatch). */
 int qcb_ildg_read(qcb_field f, const char* path);
 /* Reads the lattice extents and precision of an ILDG file ("ildg-format" record). */
 int qcb_ildg_probe(const char* path, int L[4], int* precision);
+/* SciDAC (USQCD QIO) checksums of a payload of n_sites records of site_bytes bytes in rank
+ * order, bytes as stored: c_r = CRC-32 (zlib) of record r, suma = XOR rotl(c_r, r mod 29),
+ * sumb = XOR rotl(c_r, r mod 31).  Host-only; needs no device. */
+int qcb_scidac_checksum(const void* payload, uint64_t n_sites, uint64_t site_bytes, uint32_t* suma, uint32_t* sumb);
 
 /* ------------------------------------------------------------------ instrumentation */
 /* Kernel classes timed by CUDA events recorded on the handle's stream around each launch. */

@@ -77,3 +77,53 @@ def test_ildg_probe_errors(qcb, tmp_path):
     with pytest.raises(qcb.QcbError) as e:
         qcb.ildg_probe(str(noxml))
     assert e.value.code == -4
+
+
+def scidac_sums_zlib(payload: bytes, site_bytes: int):
+    """Independent restatement of the SciDAC checksum with zlib's CRC-32."""
+    import zlib
+
+    rotl = lambda v, r: ((v << r) | (v >> (32 - r))) & 0xFFFFFFFF if r else v
+    a = b = 0
+    for r in range(len(payload) // site_bytes):
+        c = zlib.crc32(payload[r * site_bytes:(r + 1) * site_bytes])
+        a ^= rotl(c, r % 29)
+        b ^= rotl(c, r % 31)
+    return a, b
+
+
+def scidac_record(a: int, b: int) -> bytes:
+    return (f"<?xml version=\"1.0\" encoding=\"UTF-8\"?><scidacChecksum><version>1.0</version>"
+            f"<suma>{a:x}</suma><sumb>{b:x}</sumb></scidacChecksum>").encode()
+
+
+def test_scidac_checksum_known_answer(qcb):
+    # CRC-32 check value of "123456789"; one record at rank 0 is rotated by 0 in both sums
+    assert qcb.scidac_checksum(b"123456789", 9) == (0xCBF43926, 0xCBF43926)
+    assert qcb.scidac_checksum(b"", 8) == (0, 0)
+
+
+@pytest.mark.parametrize("n_sites,site_bytes", [(1, 576), (29, 576), (31, 13), (1000, 288), (20000, 24), (9000, 7)])
+def test_scidac_checksum_matches_zlib(qcb, n_sites, site_bytes):
+    import numpy as np
+
+    payload = np.random.default_rng(n_sites + site_bytes).integers(0, 256, n_sites * site_bytes, dtype=np.uint8)
+    payload = payload.tobytes()
+    assert qcb.scidac_checksum(payload, site_bytes) == scidac_sums_zlib(payload, site_bytes)
+
+
+def test_ildg_probe_scidac_record(qcb, tmp_path):
+    L = (2, 2, 2, 2)
+    body = b"\0" * (16 * 72 * 8)
+    good = tmp_path / "good"
+    good.write_bytes(lime_record(b"ildg-format", ildg_xml(L), True, True) +
+                     lime_record(b"ildg-binary-data", body, False, False) +
+                     lime_record(b"scidac-checksum", scidac_record(*scidac_sums_zlib(body, 576)), False, True))
+    assert qcb.ildg_probe(str(good)) == (L, 64)
+    bad = tmp_path / "bad"
+    bad.write_bytes(lime_record(b"ildg-format", ildg_xml(L), True, True) +
+                    lime_record(b"ildg-binary-data", body, False, False) +
+                    lime_record(b"scidac-checksum", b"<scidacChecksum><suma>zz</suma></scidacChecksum>", False, True))
+    with pytest.raises(qcb.QcbError) as e:
+        qcb.ildg_probe(str(bad))
+    assert e.value.code == -4

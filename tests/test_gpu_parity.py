@@ -237,6 +237,70 @@ def test_ildg_32bit_payload(gpu, orc, tmp_path):
     assert V * 72 * 4 == len(body)
 
 
+def test_ildg_scidac_checksum_write_and_verify(gpu, orc, tmp_path):
+    """The checksum record a write adds matches zlib's restatement over the payload; the file
+    reads back exactly; one flipped payload byte, or a wrong sum, makes the read fail."""
+    from test_abi import scidac_sums_zlib
+
+    L = (4, 6, 2, 8)
+    U = orc.hot_start(L, 12)
+    f = gpu.GaugeField(L, 64, 0)
+    f.upload(U)
+    p = tmp_path / "cfg"
+    f.save_ildg(str(p), scidac_checksum=True)
+    raw = p.read_bytes()
+    recs, off = [], 0
+    while off < len(raw):
+        _, _, flags, _, n = struct.unpack(">IHBBQ", raw[off:off + 16])
+        recs.append((raw[off + 16:off + 144].rstrip(b"\0"), flags, raw[off + 144:off + 144 + n]))
+        off += 144 + ((n + 7) // 8) * 8
+    assert [(t, fl) for t, fl, _ in recs] == [(b"ildg-format", 0xC0), (b"ildg-binary-data", 0x00),
+                                               (b"scidac-checksum", 0x40)]
+    a, b = scidac_sums_zlib(recs[1][2], 576)
+    assert f"<suma>{a:x}</suma><sumb>{b:x}</sumb>".encode() in recs[2][2]
+    g = gpu.GaugeField(L, 64, 0)
+    g.read_ildg(str(p))
+    assert np.array_equal(g.download(), U)
+    # the default write is the reference's two records: the same bytes up to the end of the
+    # binary payload, with that record ending the message (ME set) and no checksum record
+    off_bin = 144 + ((len(recs[0][2]) + 7) // 8) * 8
+    plain = bytearray(raw[:off_bin + 144 + len(recs[1][2])])
+    plain[off_bin + 6] = 0x40
+    q = tmp_path / "plain"
+    f.save_ildg(str(q))
+    assert q.read_bytes() == bytes(plain)
+    bad = bytearray(raw)
+    bad[off_bin + 144 + 1000] ^= 0x01  # inside the binary payload
+    (tmp_path / "bad").write_bytes(bytes(bad))
+    with pytest.raises(gpu.QcbError) as e:
+        g.read_ildg(str(tmp_path / "bad"))
+    assert e.value.code == -4
+
+
+def test_ildg_scidac_checksum_32bit_interop(gpu, orc, tmp_path):
+    """A 32-bit file written outside the library with a zlib-computed checksum is accepted, and
+    rejected once its sum is wrong."""
+    from test_abi import ildg_xml, lime_record, scidac_record, scidac_sums_zlib
+
+    L = (4, 4, 2, 4)
+    U = orc.hot_start(L, 6)
+    body = U.view(np.float64).astype(">f4").tobytes()
+    a, b = scidac_sums_zlib(body, 288)
+    for sums, ok in [((a, b), True), ((a ^ 1, b), False)]:
+        p = tmp_path / f"c32_{ok}"
+        p.write_bytes(lime_record(b"ildg-format", ildg_xml(L, 32), True, True) +
+                      lime_record(b"ildg-binary-data", body, False, False) +
+                      lime_record(b"scidac-checksum", scidac_record(*sums), False, True))
+        f = gpu.GaugeField(L, 64, 0)
+        if ok:
+            f.read_ildg(str(p))
+            assert np.max(np.abs(f.download() - U)) < 1e-7
+        else:
+            with pytest.raises(gpu.QcbError) as e:
+                f.read_ildg(str(p))
+            assert e.value.code == -4
+
+
 def test_invalid_arguments(gpu):
     with pytest.raises(gpu.QcbError) as e:
         gpu.GaugeField((5, 4, 4, 4))
