@@ -17,6 +17,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libqcb.so")
+# the same library with every field index validated on the device (QCB_CHECKED)
+CHECKED_LIB_PATH = os.path.join(HERE, "libqcb_checked.so")
 
 PREC_F64, PREC_F32 = 64, 32
 STORE_18, STORE_12 = 0, 1
@@ -79,6 +81,8 @@ def exported_symbols():
         "qcb_ildg_probe": (i, [C.c_char_p, _i4, pi]),
         "qcb_ildg_write_ex": (i, [_vp, C.c_char_p, i]),
         "qcb_scidac_checksum": (i, [_vp, u64, u64, C.POINTER(u32), C.POINTER(u32)]),
+        "qcb_debug_oob": (i, [pi, C.POINTER(u64), C.POINTER(u64)]),
+        "qcb_debug_probe_link": (i, [_vp, i, i, C.c_int64]),
         "qcb_timing_enable": (i, [_vp, i]),
         "qcb_timing_read": (i, [_vp, i, C.POINTER(C.c_long), pd]),
         "qcb_timing_reset": (i, [_vp]),
@@ -252,6 +256,9 @@ class GaugeField:
         _check(lib().qcb_diag_staple(self.h, int(mu), out.ctypes.data))
         return out
 
+    def debug_probe_link(self, mu: int, parity: int, h: int) -> None:
+        _check(lib().qcb_debug_probe_link(self.h, int(mu), int(parity), int(h)))
+
     # -- ILDG
     def save_ildg(self, path: str, scidac_checksum: bool = False) -> None:
         if scidac_checksum:
@@ -404,6 +411,13 @@ def ildg_probe(path: str):
     p = C.c_int()
     _check(lib().qcb_ildg_probe(os.fsencode(path), L, C.byref(p)))
     return tuple(int(v) for v in L), p.value
+
+
+def debug_oob():
+    """(checked build?, out-of-bounds access count, first bad access) since the last call."""
+    c, n, f = C.c_int(), C.c_uint64(), C.c_uint64()
+    _check(lib().qcb_debug_oob(C.byref(c), C.byref(n), C.byref(f)))
+    return bool(c.value), n.value, f.value
 
 
 def scidac_checksum(payload, site_bytes: int):

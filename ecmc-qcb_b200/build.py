@@ -3,7 +3,10 @@
     python ecmc-qcb_b200/build.py [-v]
 
 Each translation unit under csrc/ is compiled to _build/*.o in parallel and linked
-into ecmc-qcb_b200/libqcb.so.  Objects are rebuilt when a source or header is newer.
+into ecmc-qcb_b200/libqcb.so; the same sources compiled with -DQCB_CHECKED into
+_build/checked/*.o give libqcb_checked.so, whose kernels validate every field index
+(the out-of-bounds record of qcb_debug_oob).  Objects are rebuilt when a source or
+header is newer.
 """
 from __future__ import annotations
 
@@ -17,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libqcb.so")
+CHECKED_LIB = os.path.join(HERE, "libqcb_checked.so")
 HOST = os.path.join(HERE, "host", "src")
 COMPAT = os.path.join(HERE, "libqcb_compat.a")
 DRIVER = os.path.join(HERE, "qcb_hb_cb")
@@ -34,12 +38,13 @@ def _deps_mtime() -> float:
     return max(os.path.getmtime(h) for h in hs) if hs else 0.0
 
 
-def _compile(src: str, verbose: bool) -> str:
-    obj = os.path.join(BUILD, os.path.basename(src).rsplit(".", 1)[0] + ".o")
+def _compile(src: str, verbose: bool, checked: bool = False) -> str:
+    out = os.path.join(BUILD, "checked") if checked else BUILD
+    obj = os.path.join(out, os.path.basename(src).rsplit(".", 1)[0] + ".o")
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), _deps_mtime()):
         return obj
-    cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
-    if verbose:
+    cmd = [NVCC, *ARCH, *FLAGS, *(["-DQCB_CHECKED"] if checked else []), "-c", src, "-o", obj]
+    if verbose and not checked:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -49,16 +54,22 @@ def _compile(src: str, verbose: bool) -> str:
     return obj
 
 
-def build(verbose: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
-    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
-    with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs, "-ccbin", "/usr/bin/g++"]
+def _link(lib: str, objs: list) -> None:
+    if not os.path.exists(lib) or os.path.getmtime(lib) < max(os.path.getmtime(o) for o in objs):
+        cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", lib, *objs, "-ccbin", "/usr/bin/g++"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
-            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+            raise RuntimeError(f"link of {os.path.basename(lib)} failed:\n{r.stdout}\n{r.stderr}")
+
+
+def build(verbose: bool = False) -> str:
+    os.makedirs(os.path.join(BUILD, "checked"), exist_ok=True)
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    jobs = [(s, False) for s in srcs] + [(s, True) for s in srcs]
+    with cf.ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 8)) as ex:
+        objs = list(ex.map(lambda j: _compile(j[0], verbose, j[1]), jobs))
+    _link(LIB, objs[:len(srcs)])
+    _link(CHECKED_LIB, objs[len(srcs):])
     build_host()
     return LIB
 

@@ -326,11 +326,64 @@ int qcb::field_download_host(qcb_field_s* f, double* host, int bswap) {
     return QCB_OK;
 }
 
+#ifdef QCB_CHECKED
+// Every translation unit of the checked build registers the reader of its out-of-bounds record.
+namespace qcb {
+static std::vector<OobTake>& oob_registry() {
+    static std::vector<OobTake> v;
+    return v;
+}
+void register_oob(OobTake fn) { oob_registry().push_back(fn); }
+}  // namespace qcb
+#endif
+
 // ====================================================================== C ABI
 extern "C" {
 
 const char* qcb_last_error(void) { return g_err.c_str(); }
+#ifdef QCB_CHECKED
+const char* qcb_version(void) { return "qcb 0.1 (sm_100a, checked)"; }
+#else
 const char* qcb_version(void) { return "qcb 0.1 (sm_100a)"; }
+#endif
+
+int qcb_debug_oob(int* checked, uint64_t* count, uint64_t* first) {
+    if (!checked || !count || !first) return fail(QCB_EINVAL, "null argument");
+    *count = 0;
+    *first = 0;
+#ifdef QCB_CHECKED
+    *checked = 1;
+    CK(cudaDeviceSynchronize());
+    for (OobTake fn : oob_registry()) {
+        unsigned long long c = 0, f0 = 0;
+        const cudaError_t e = fn(&c, &f0);
+        if (e == cudaErrorInvalidSymbol) {  // a unit without device code keeps no record
+            cudaGetLastError();
+            continue;
+        }
+        CK(e);
+        if (c && !*count) *first = f0;
+        *count += c;
+    }
+#else
+    *checked = 0;
+#endif
+    return QCB_OK;
+}
+
+int qcb_debug_probe_link(qcb_field f, int mu, int parity, int64_t h) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+#ifndef QCB_CHECKED
+    // only the checked build may send an index outside the field to the device, where its own
+    // check catches it
+    if (mu < 0 || mu > 3 || parity < 0 || parity > 1 || h < 0 || h >= f->g.Vh)
+        return fail(QCB_EINVAL, "probe: (mu, parity, h) outside the field");
+#endif
+    if (h < INT32_MIN || h > INT32_MAX) return fail(QCB_EINVAL, "probe: h outside the int range");
+    return launch(f, QCB_K_OTHER, [&] {
+        return fmt_ops(f->fmt).probe_link(f->g, f->links, mu, parity, (int)h, f->d_res, f->stream);
+    });
+}
 uint64_t qcb_launch_count(void) { return g_launches.load(); }
 
 int qcb_field_create(const int L[4], int prec, int store, qcb_field* out) {

@@ -24,6 +24,49 @@
 
 namespace qcb {
 
+#ifdef QCB_CHECKED
+// Checked build (libqcb_checked.so): every (mu, parity, h) that a link or algebra access is
+// formed from is validated on the device before the address is.  A bad one is counted in this
+// translation unit's record, the first is kept as kind << 62 | (mu & 63) << 56 | (par & 255) << 48
+// | (h mod 2^48) (kind 0 = link, 1 = su(3) algebra), and the access is redirected to link
+// (0, 0, 0), inside the allocation, so the kernel runs on instead of faulting.  The host reads
+// and clears every translation unit's record through qcb_debug_oob.
+static __device__ unsigned long long g_oob_count;
+static __device__ unsigned long long g_oob_first;
+static __device__ __noinline__ void note_oob(int kind, int mu, int par, int64_t h) {
+    const unsigned long long key = ((unsigned long long)kind << 62) | ((unsigned long long)(mu & 63) << 56) |
+                                   ((unsigned long long)(par & 255) << 48) |
+                                   ((unsigned long long)h & 0xFFFFFFFFFFFFull);
+    if (atomicAdd(&g_oob_count, 1ull) == 0ull) g_oob_first = key;
+}
+typedef cudaError_t (*OobTake)(unsigned long long* count, unsigned long long* first);
+void register_oob(OobTake fn);  // the registry lives in qcb_api.cu
+// This translation unit's record, read and cleared (invalid-symbol when the unit has no kernels).
+static cudaError_t oob_take(unsigned long long* count, unsigned long long* first) {
+    cudaError_t e = cudaMemcpyFromSymbol(count, g_oob_count, sizeof(*count));
+    if (e == cudaSuccess) e = cudaMemcpyFromSymbol(first, g_oob_first, sizeof(*first));
+    const unsigned long long zero = 0;
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_oob_count, &zero, sizeof(zero));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_oob_first, &zero, sizeof(zero));
+    return e;
+}
+static const int g_oob_registered = (register_oob(&oob_take), 0);
+#endif
+
+// Validates (mu, par, h) of a field access in the checked build (see above); a no-op otherwise.
+QCB_HD void check_index(int kind, int& mu, int& par, int& h, int64_t Vh) {
+#if defined(QCB_CHECKED) && defined(__CUDA_ARCH__)
+    if (!((unsigned)mu < 4u && (unsigned)par < 2u && h >= 0 && (int64_t)h < Vh)) {
+        note_oob(kind, mu, par, h);
+        mu = 0;
+        par = 0;
+        h = 0;
+    }
+#else
+    (void)kind, (void)mu, (void)par, (void)h, (void)Vh;
+#endif
+}
+
 template <typename R>
 struct V2;
 template <>
@@ -155,6 +198,7 @@ struct LinkField {
     static constexpr int kPairs = kQuad ? NE / 2 : 0;
     // start of the tile holding link (mu, par, h)
     QCB_HD size_t tile0(int mu, int par, int h) const {
+        check_index(0, mu, par, h, Vh);
         const int nT = (int)((Vh + 31) >> 5);
         return (size_t)((mu * 2 + par) * nT + (h >> 5)) * (NE * 32);
     }
@@ -162,6 +206,7 @@ struct LinkField {
     QCB_HD int64_t es() const { return TILED ? 32 : Vh; }
     QCB_HD size_t index0(int mu, int par, int h) const {
         if (TILED) return tile0(mu, par, h) + (h & 31);
+        check_index(0, mu, par, h, Vh);
         return (size_t)((mu * 2 + par) * NE) * (size_t)Vh + (size_t)h;
     }
     template <bool RO>
@@ -253,6 +298,7 @@ struct AlgField {
     C2* p;
     int64_t Vh;
     QCB_HD size_t tile0(int mu, int par, int h) const {
+        check_index(1, mu, par, h, Vh);
         const int nT = (int)((Vh + 31) >> 5);
         return (size_t)((mu * 2 + par) * nT + (h >> 5)) * (4 * 32);
     }

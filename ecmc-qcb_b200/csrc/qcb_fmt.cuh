@@ -90,6 +90,11 @@ struct FmtImpl {
             default: return hb1_mu<3>(g, links, par, c_alpha, n_hits, seed, sweep, rep, err, s);
         }
     }
+    static cudaError_t probe_link(const Geom& g, const void* links, int mu, int par, int h, double* out,
+                                  cudaStream_t s) {
+        k_probe_link<R, NE><<<1, 1, 0, s>>>(view(links, g.Vh), mu, par, h, out);
+        return cudaGetLastError();
+    }
     static cudaError_t flow1(const Geom& g, const void* win, void* wout, void* z, double eps, int stage, int rep,
                              cudaStream_t s) {
         const unsigned nb = 8u * (unsigned)((g.Vh + QCB_FLOW1_THREADS - 1) / QCB_FLOW1_THREADS);
@@ -170,6 +175,7 @@ struct FmtImpl {
         o.plaq_tiles = &plaq_tiles;
         o.clover_tiles = &clover_tiles;
         o.hb1 = &hb1;
+        o.probe_link = &probe_link;
         o.flow1 = &flow1;
         o.plaquette = &plaquette;
         o.clover = &clover;

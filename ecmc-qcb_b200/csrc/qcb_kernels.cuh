@@ -1051,6 +1051,14 @@ __global__ void k_reunitarize(Geom g, LinkField<R, NE> U) {
 }
 
 // Staple field of one direction, written in AoS order (diagnostic entry point).
+// Loads one link (mu, par, h) and stores its trace: the probe through which a test shows the
+// checked build catching an index outside the field.
+template <typename R, int NE>
+__global__ void k_probe_link(LinkField<R, NE> U, int mu, int par, int h, double* out) {
+    const M3<R> u = U.load(mu, par, h);
+    out[0] = (double)(u(0, 0).re + u(1, 1).re + u(2, 2).re);
+}
+
 template <typename R, int NE, int MU>
 __global__ void k_staple_field(Geom g, LinkField<R, NE> U, double2* out) {
     const int par = blockIdx.y;

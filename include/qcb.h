@@ -160,6 +160,19 @@ int qcb_timing_enable(qcb_field f, int on);
 int qcb_timing_read(qcb_field f, int kclass, long* launches, double* total_ms);
 int qcb_timing_reset(qcb_field f);
 
+/* ------------------------------------------------------------------ checked build */
+/* libqcb_checked.so is this library built with QCB_CHECKED: every (mu, parity, h) that a link
+ * or su(3)-algebra access is formed from is validated on the device first; a bad one is counted,
+ * the first kept, and the access redirected inside the field, so a kernel with an indexing error
+ * reports it instead of faulting.  qcb_debug_oob synchronises the device and returns (and clears)
+ * the count and the first bad access, packed as kind << 62 | (mu & 63) << 56 | (parity & 255) << 48
+ * | (h mod 2^48) with kind 0 = link, 1 = algebra; *checked is 0 (and the count 0) in the normal
+ * build. */
+int qcb_debug_oob(int* checked, uint64_t* count, uint64_t* first);
+/* Loads link (mu, parity, h) in a one-thread kernel.  The normal build rejects an index outside
+ * the field on the host (QCB_EINVAL); the checked build passes it to the device check. */
+int qcb_debug_probe_link(qcb_field f, int mu, int parity, int64_t h);
+
 /* ------------------------------------------------------------------ diagnostics */
 /* Staple A(x, mu) of every site (src/gauge/GaugeField.cpp:74-97) into host AoS (V*9 complex). */
 int qcb_diag_staple(qcb_field f, int mu, double* out);

@@ -127,3 +127,14 @@ def test_ildg_probe_scidac_record(qcb, tmp_path):
     with pytest.raises(qcb.QcbError) as e:
         qcb.ildg_probe(str(bad))
     assert e.value.code == -4
+
+
+def test_checked_library_exports_every_declared_symbol(qcb):
+    import ctypes
+
+    assert os.path.exists(qcb.CHECKED_LIB_PATH), "build() also makes libqcb_checked.so"
+    lib = ctypes.CDLL(qcb.CHECKED_LIB_PATH)
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+    lib.qcb_version.restype = ctypes.c_char_p
+    assert b"checked" in lib.qcb_version() and b"checked" not in qcb.lib().qcb_version()
