@@ -524,11 +524,51 @@ def run_serve(qcb, n_req: int, stores=(0, 1), low_rates=(4.0, 2.0), n_low: int =
     return out
 
 
+def capture_batch(qcb, args):
+    """A quarter of the batching configuration (same mix of 8^4 ... 24^4 chains and couplings,
+    1.5 GB FP64) for ncu captures of the tiled heatbath: 12-real storage and launch shape 0 (the
+    tuner's usual choice on the full batch), `warmup` untimed then `steps` CUDA-graph sweeps."""
+    import numpy as np
+
+    rng = np.random.default_rng(0)
+    Ls = [(8,) * 4] * 24 + [(12,) * 4] * 24 + [(16,) * 4] * 12 + [(24,) * 4] * 4
+    b = qcb.Batch(Ls, rng.uniform(5.7, 6.3, len(Ls)), list(range(len(Ls))), qcb.PREC_F64, qcb.STORE_12)
+    b.hot_start()
+    b.set_variant(0)
+    b.sweep(1, args.warmup)
+    b.sweep(1, args.steps)
+    b.sync()
+    b.close()
+
+
+def capture_serve(qcb, args):
+    """24 serving requests of 16^4 (FP32-18, 1.1 GB resident), all on the shared tiled path, each
+    flowed `steps` RK3 steps, for ncu captures of the shared flow stage and clover pass.  The inputs
+    are made before the server starts and submitted back to back, so with a few hundred steps all
+    24 requests are resident together after the first ticks."""
+    f = qcb.GaugeField((16,) * 4)
+    inputs = []
+    for rid in range(24):
+        f.hot_start(1000 + rid)
+        inputs.append(f.download())
+    f.close()
+    srv = qcb.Server(150 << 30, qcb.PREC_F32, qcb.STORE_18)
+    for rid, U in enumerate(inputs):
+        srv.submit(rid, (16,) * 4, U, 0.02, args.steps)
+    srv.wait(600.0)
+    while srv.poll() is not None:
+        pass
+    srv.close()
+
+
 def run_ours(args, rank: int, world: int, local: int):
     import torch
 
     qcb = load_package()
     torch.cuda.set_device(local)
+    if args.only in ("batch", "serve"):
+        (capture_batch if args.only == "batch" else capture_serve)(qcb, args)
+        return
     hbm_peak, peak_kind = peaks()
     V = L[0] * L[1] * L[2] * L[3]
     f = qcb.GaugeField(L, qcb.PREC_F64, qcb.STORE_18)
@@ -697,7 +737,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="length of the CPU-baseline sample (0 skips it)")
-    ap.add_argument("--only", default="all", choices=["all", "hb", "flow", "obs"],
+    ap.add_argument("--only", default="all", choices=["all", "hb", "flow", "obs", "batch", "serve"],
                     help="run one part (used for ncu captures of a single kernel family)")
     ap.add_argument("--parts", default="all", choices=["all", "core"],
                     help="core: skip the batch and serving sections")
