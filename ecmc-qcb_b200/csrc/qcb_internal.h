@@ -53,7 +53,6 @@ struct qcb_field_s {
     double* d_res = nullptr;  // device results (8 doubles)
     double* h_res = nullptr;  // pinned host results (8 doubles)
     int* d_err = nullptr;     // device error flags
-    int hb_variant = 1;  // heatbath launch shape (index into the autotuner's candidates)
     bool timing = false;
     std::vector<qcb::TimedLaunch> pending;
     std::vector<cudaEvent_t> event_pool;
