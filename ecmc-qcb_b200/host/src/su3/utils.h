@@ -1,7 +1,7 @@
 // su3/utils.h -- host-side SU(3) value type of the C++ compatibility layer.
 //
 // The reference's SU3 is Eigen::Matrix<std::complex<double>,3,3,RowMajor> (src/su3/utils.h:12);
-// Eigen is not part of this build, so SU3 here is a small row-major 3x3 complex value type with
+// Eigen is not used here, so SU3 here is a small row-major 3x3 complex value type with
 // the operations host code applies to individual links (element access, products, adjoint,
 // trace).  SU3Map is the writable view into a field's host links that GaugeField::view_link
 // returns (src/gauge/GaugeField.h:49-56).

@@ -1,6 +1,6 @@
 """ctypes binding of the CPU oracle (test infrastructure only).
 
-This module is the checker: only tests/, __graft_entry__.smoke() and the
+The oracle checks the CUDA product: only tests/, __graft_entry__.smoke() and the
 cpu_baseline / reference legs of bench.py import it.  The product
 (ecmc-qcb_b200/) never does.  Parity is unpinned by reference fixtures (the
 reference ships none and cannot be compiled in this image); the restatement

@@ -1,8 +1,8 @@
 /*
  * qcb_oracle.h -- CPU restatement of the ECMC-QCB gauge-field hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA
- * product in ecmc-qcb_b200/: only tests/, __graft_entry__.smoke() and the
+ * TEST INFRASTRUCTURE ONLY.  This library is the oracle the CUDA product in
+ * ecmc-qcb_b200/ is checked against: only tests/, __graft_entry__.smoke() and the
  * cpu_baseline / --impl reference legs of bench.py may load it.  Nothing in
  * the product links or calls it.
  *

@@ -1,7 +1,7 @@
 """CUDA path vs the CPU oracle and the golden fixtures, FP64 builds, through the C ABI.
 
-Tolerance: 1e-12 relative (north-star (a)/(b)); Q, being a signed sum near zero, is compared
-with an absolute bound of 1e-12 * max(1, sum_x |q(x)|).
+Tolerance: 1e-12 relative (links, plaquette, E and the heatbath updates); Q, being a signed sum
+near zero, is compared with an absolute bound of 1e-12 * max(1, sum_x |q(x)|).
 """
 import os
 import struct
@@ -106,7 +106,7 @@ def test_hot_start_matches_oracle(gpu, orc, L):
 
 @pytest.mark.parametrize("L,nh", [((8, 8, 8, 8), 2), ((4, 6, 2, 8), 1)])
 def test_heatbath_harness_link_by_link(gpu, orc, L, nh):
-    """North-star (b): every (parity, mu) update, fed the same input and the same Philox draws as
+    """Every (parity, mu) update, fed the same input and the same Philox draws as
     the oracle's restatement of the reference's update routine, matches link by link to 1e-12."""
     U = orc.hot_start(L, 99)
     f = gpu.GaugeField(L, 64, 0)

@@ -6,7 +6,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-DQ_MAX = 1e-4  # |Q_fp32 - Q_fp64| (north-star target)
+DQ_MAX = 1e-4  # bound on |Q_fp32 - Q_fp64|
 DE_REL_MAX = 1e-6  # |E_fp32 - E_fp64| / E_fp64
 DP_MAX = 1e-6  # |P_fp32 - P_fp64|
 
@@ -50,7 +50,7 @@ def binned_mean(x, nbin=10):
 
 
 def test_independent_chains_reproduce_oracle_plaquette(gpu, orc):
-    """North-star (c): <P> of independent GPU chains at beta = 6.0 agrees with independent oracle
+    """<P> of independent GPU chains at beta = 6.0 agrees with independent oracle
     chains within 2 sigma, and the links stay unitary to 1e-12 without reprojection.  Both sides
     start cold, thermalise 100 sweeps and measure 500; errors come from bins of 50 sweeps (many
     autocorrelation times of the plaquette) combined over 4 oracle and 32 GPU chains."""

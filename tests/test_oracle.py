@@ -14,7 +14,7 @@ import scipy.linalg as sla
 from conftest import rel_err
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden_4444.npz")
-TOL = 1e-12  # FP64 parity tolerance (relative), north-star (a)
+TOL = 1e-12  # FP64 parity tolerance (relative)
 
 
 @pytest.fixture(scope="module")
@@ -203,7 +203,7 @@ def test_heatbath_unitarity_and_acceptance(orc):
     for sweep in range(20):
         orc.hb_sweep(U, L, 6.0, 1, 12345, sweep)
     mx, _ = orc.unitarity(U, L)
-    assert mx < 1e-12  # north-star (c): ||U^dag U - 1|| < 1e-12 without reprojection
+    assert mx < 1e-12  # ||U^dag U - 1|| < 1e-12 without reprojection
     assert 0.55 < orc.plaquette(U, L) < 0.65
 
 
