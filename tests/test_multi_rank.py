@@ -65,3 +65,24 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
 
     assert bench.run_reference(Args, rank=1, world=2) is None
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_json_line():
+    """The reference arm prints one JSON line with the bench contract's keys, timing the oracle's
+    heatbath on the host cores for the same workload, metric and unit as the CUDA arm."""
+    import json
+    import subprocess
+
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "3"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "link-upd/s" and d["value"] > 0
+    assert d["steps"] == 1 and d["warmup"] == 3 and d["n_gpus"] == 1 and d["higher_is_better"] is True
+    assert d["config"]["workload"] == "hb_fp64_32^4" and d["dtype"] == "f64" and d["vs_baseline"] is None
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "link-upd/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
