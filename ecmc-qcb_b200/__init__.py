@@ -82,6 +82,8 @@ def exported_symbols():
         "qcb_ildg_write_ex": (i, [_vp, C.c_char_p, i]),
         "qcb_scidac_checksum": (i, [_vp, u64, u64, C.POINTER(u32), C.POINTER(u32)]),
         "qcb_debug_oob": (i, [pi, C.POINTER(u64), C.POINTER(u64)]),
+        "qcb_field_prefetch_aos": (i, [_vp, _vp]),
+        "qcb_field_commit_prefetch": (i, [_vp]),
         "qcb_debug_probe_link": (i, [_vp, i, i, C.c_int64]),
         "qcb_timing_enable": (i, [_vp, i]),
         "qcb_timing_read": (i, [_vp, i, C.POINTER(C.c_long), pd]),
@@ -184,6 +186,20 @@ class GaugeField:
         out = np.empty((self.V, 4, 3, 3), dtype=np.complex128)
         _check(lib().qcb_field_download_aos(self.h, out.ctypes.data))
         return out
+
+    def prefetch(self, U: np.ndarray) -> None:
+        """Starts the pipelined upload of U (pageable: staged before this returns); the links
+        change at commit_prefetch()."""
+        U = np.ascontiguousarray(U, dtype=np.complex128)
+        _check(lib().qcb_field_prefetch_aos(self.h, U.ctypes.data))
+
+    def prefetch_ptr(self, host_ptr: int) -> None:
+        """Pipelined upload from a host pointer (pinned memory: asynchronous; keep the buffer
+        unchanged until a synchronising call after the commit)."""
+        _check(lib().qcb_field_prefetch_aos(self.h, _vp(host_ptr)))
+
+    def commit_prefetch(self) -> None:
+        _check(lib().qcb_field_commit_prefetch(self.h))
 
     def upload_device_ptr(self, ptr: int) -> None:
         _check(lib().qcb_field_upload_aos_device(self.h, _vp(ptr)))

@@ -113,6 +113,21 @@ int ensure_staging(qcb_field_s* f) {
     CK(cudaMalloc(&f->staging, (size_t)f->g.V * 36 * sizeof(double2)));
     return QCB_OK;
 }
+// The staging buffer for a use on the field's stream; refused while a prefetched configuration
+// occupies it.
+int staging_acquire(qcb_field_s* f) {
+    if (f->prefetch_pending)
+        return fail(QCB_EINVAL, "a prefetched configuration occupies the staging buffer: commit it first");
+    return ensure_staging(f);
+}
+// Marks the end of the staging buffer's latest use on the field's stream: the next prefetch copy
+// waits for this point only, not for everything queued on the stream after it.
+int staging_release(qcb_field_s* f) {
+    if (!f->ev_staging) CK(cudaEventCreateWithFlags(&f->ev_staging, cudaEventDisableTiming));
+    CK(cudaEventRecord(f->ev_staging, f->stream));
+    f->staging_used = true;
+    return QCB_OK;
+}
 int ensure_alt(qcb_field_s* f) {
     if (f->alt) return QCB_OK;
     CK(cudaMalloc(&f->alt, link_bytes(f->fmt, f->g.Vh)));
@@ -312,16 +327,18 @@ __global__ void k_diag_philox(uint4 ctr, uint2 key, int n, uint4* out) {
 }  // namespace
 
 int qcb::field_upload_host(qcb_field_s* f, const double* host, int bswap) {
-    RET(ensure_staging(f));
+    RET(staging_acquire(f));
     CK(cudaMemcpyAsync(f->staging, host, (size_t)f->g.V * 36 * sizeof(double2), cudaMemcpyHostToDevice, f->stream));
     RET(upload_from_staging(f, bswap));
+    RET(staging_release(f));
     CK(cudaStreamSynchronize(f->stream));
     return QCB_OK;
 }
 int qcb::field_download_host(qcb_field_s* f, double* host, int bswap) {
-    RET(ensure_staging(f));
+    RET(staging_acquire(f));
     RET(download_to_staging(f, bswap));
     CK(cudaMemcpyAsync(host, f->staging, (size_t)f->g.V * 36 * sizeof(double2), cudaMemcpyDeviceToHost, f->stream));
+    RET(staging_release(f));
     CK(cudaStreamSynchronize(f->stream));
     return QCB_OK;
 }
@@ -398,6 +415,12 @@ int qcb_field_destroy(qcb_field f) {
         cudaEventDestroy(t.b);
     }
     for (auto e : f->event_pool) cudaEventDestroy(e);
+    if (f->copy_stream) {
+        cudaStreamSynchronize(f->copy_stream);
+        cudaStreamDestroy(f->copy_stream);
+    }
+    if (f->ev_copied) cudaEventDestroy(f->ev_copied);
+    if (f->ev_staging) cudaEventDestroy(f->ev_staging);
     if (f->links) cudaFree(f->links);
     if (f->alt) cudaFree(f->alt);
     if (f->staging) cudaFree(f->staging);
@@ -441,6 +464,29 @@ int qcb_field_upload_aos(qcb_field f, const double* links) {
     if (!f || !links) return fail(QCB_EINVAL, "null argument");
     return field_upload_host(f, links, 0);
 }
+int qcb_field_prefetch_aos(qcb_field f, const double* links) {
+    if (!f || !links) return fail(QCB_EINVAL, "null argument");
+    if (f->prefetch_pending) return fail(QCB_EINVAL, "a prefetched configuration is pending: commit it first");
+    RET(ensure_staging(f));
+    if (!f->copy_stream) {
+        CK(cudaStreamCreateWithFlags(&f->copy_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&f->ev_copied, cudaEventDisableTiming));
+    }
+    if (f->staging_used) CK(cudaStreamWaitEvent(f->copy_stream, f->ev_staging, 0));
+    CK(cudaMemcpyAsync(f->staging, links, (size_t)f->g.V * 36 * sizeof(double2), cudaMemcpyHostToDevice,
+                       f->copy_stream));
+    CK(cudaEventRecord(f->ev_copied, f->copy_stream));
+    f->prefetch_pending = true;
+    return QCB_OK;
+}
+int qcb_field_commit_prefetch(qcb_field f) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    if (!f->prefetch_pending) return fail(QCB_EINVAL, "no prefetched configuration to commit");
+    CK(cudaStreamWaitEvent(f->stream, f->ev_copied, 0));
+    f->prefetch_pending = false;
+    RET(upload_from_staging(f, 0));
+    return staging_release(f);
+}
 int qcb_field_download_aos(qcb_field f, double* links) {
     if (!f || !links) return fail(QCB_EINVAL, "null argument");
     return field_download_host(f, links, 0);
@@ -473,10 +519,11 @@ int qcb_field_copy(qcb_field dst, qcb_field src) {
                            dst->stream));
         return QCB_OK;
     }
-    RET(ensure_staging(dst));
+    RET(staging_acquire(dst));
     RET(launch(dst, QCB_K_OTHER,
                [&] { return fmt_ops(src->fmt).soa_to_aos(src->g, src->links, dst->staging, 0, dst->stream); }));
-    return upload_from_staging(dst, 0);
+    RET(upload_from_staging(dst, 0));
+    return staging_release(dst);
 }
 
 int qcb_cold_start(qcb_field f) {
@@ -693,10 +740,11 @@ int qcb_timing_reset(qcb_field f) {
 // ------------------------------------------------------------------ diagnostics
 int qcb_diag_staple(qcb_field f, int mu, double* out) {
     if (!f || !out || mu < 0 || mu > 3) return fail(QCB_EINVAL, "invalid argument");
-    RET(ensure_staging(f));
+    RET(staging_acquire(f));
     RET(launch(f, QCB_K_OTHER,
                [&] { return fmt_ops(f->fmt).staple_field(f->g, f->links, mu, f->staging, f->stream); }));
     CK(cudaMemcpyAsync(out, f->staging, (size_t)f->g.V * 9 * sizeof(double2), cudaMemcpyDeviceToHost, f->stream));
+    RET(staging_release(f));
     CK(cudaStreamSynchronize(f->stream));
     return QCB_OK;
 }

@@ -46,6 +46,11 @@ struct qcb_field_s {
     void* links = nullptr;  // current link buffer
     void* alt = nullptr;    // second link buffer (shift target), lazily allocated
     double2* staging = nullptr;  // device AoS staging buffer, lazily allocated
+    cudaStream_t copy_stream = nullptr;  // host -> staging copies of qcb_field_prefetch_aos
+    cudaEvent_t ev_copied = nullptr;     // end of the latest prefetch copy
+    cudaEvent_t ev_staging = nullptr;    // end of the staging buffer's latest use on `stream`
+    bool staging_used = false;           // ev_staging has been recorded
+    bool prefetch_pending = false;       // a prefetched configuration waits in staging for its commit
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     double* partials = nullptr;

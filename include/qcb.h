@@ -69,6 +69,18 @@ int qcb_field_sync(qcb_field f);
  * (src/gauge/GaugeField.h:27).  `links` may be pageable or pinned host memory. */
 int qcb_field_upload_aos(qcb_field f, const double* links);
 int qcb_field_download_aos(qcb_field f, double* links);
+/* Pipelined upload.  qcb_field_prefetch_aos starts copying an AoS configuration into the field's
+ * staging buffer on a copy stream of its own and returns; the copy overlaps whatever the field's
+ * stream is running (the links are not touched).  qcb_field_commit_prefetch then enqueues, on the
+ * field's stream, the conversion of the copied configuration into the links, after the copy ends.
+ * From pinned memory the copy is asynchronous, and the host buffer must stay unchanged until a
+ * call after the commit has synchronised the field (qcb_field_sync, or any call that returns a
+ * result); from pageable memory the copy is staged before the prefetch returns.  While a
+ * prefetched configuration waits for its commit, the calls that need the staging buffer
+ * (qcb_field_upload_aos / download_aos, a second prefetch, ILDG I/O, a copy between formats)
+ * return QCB_EINVAL. */
+int qcb_field_prefetch_aos(qcb_field f, const double* links);
+int qcb_field_commit_prefetch(qcb_field f);
 /* Same, from / to device memory (AoS doubles already on the field's device). */
 int qcb_field_upload_aos_device(qcb_field f, const double* d_links);
 int qcb_field_download_aos_device(qcb_field f, double* d_links);
