@@ -210,8 +210,8 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
 }
 
 // Launch shapes (measured on B200, 32^4): 128-thread blocks.  Minimum resident blocks per SM:
-// heatbath 4 for FP64 (<= 128 registers; 0.206 ms a sub-sweep at N_hits = 2, 5 and 6 blocks are
-// slower, 64-thread blocks at 8 per SM within 1%) and 6 for FP32; flow stages 3 for FP64 (<= 168 registers; 4 is no faster) and 6 for FP32
+// heatbath 4 for FP64 (<= 128 registers; 0.206 ms a sub-sweep at N_hits = 2; 3, 5 and 6 blocks
+// are slower, 64-thread blocks at 8 per SM within 1%) and 6 for FP32; flow stages 3 for FP64 (<= 168 registers; 4 is no faster) and 6 for FP32
 // (<= 80 registers, no spills: 0.36 ms a stage against 0.40 ms at 4 and 0.37 ms at 8).
 #ifndef QCB_HB_THREADS
 #define QCB_HB_THREADS 128
