@@ -528,7 +528,7 @@ __device__ __forceinline__ void hb_link(const Geom& g, const LinkField<R, NE>& U
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
     const int lex = lex_of(g, c);
-    const LinkStream rng(seed, (uint32_t)(lex * 4 + MU), sweep, TAG_HB);
+    const LinkStream rng(seed, (uint32_t)lex * 4u + (uint32_t)MU, sweep, TAG_HB);  // mod 2^32, as the oracle
     M3<R> u;
     if constexpr (SLOT) {
         const StapleSlot<R> S{slot, slot_stride}, Us{slot + 9 * slot_stride, slot_stride};
@@ -995,7 +995,7 @@ __global__ void k_start(Geom g, LinkField<R, NE> U, int hot, uint64_t seed) {
         int c[4];
         site_coords(g, par, (uint32_t)h, c);
         const int lex = lex_of(g, c);
-        LinkStream rng(seed, (uint32_t)(lex * 4 + mu), 0u, TAG_HOT);
+        LinkStream rng(seed, (uint32_t)lex * 4u + (uint32_t)mu, 0u, TAG_HOT);
         double gs[12];
 #pragma unroll
         for (int k = 0; k < 12; k += 2) {
