@@ -1073,7 +1073,7 @@ __global__ void k_staple_field(Geom g, LinkField<R, NE> U, double2* out) {
         double2 v;
         v.x = (double)A.e[e].re;
         v.y = (double)A.e[e].im;
-        out[lex * 9 + e] = v;
+        out[(int64_t)lex * 9 + e] = v;
     }
 }
 
