@@ -58,9 +58,13 @@ def load_oracle():
 
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(p):
-        d = json.load(open(p))
-        return float(d["hbm_gbs"]), "measured"
+    try:
+        with open(p) as fh:
+            v = float(json.load(fh)["hbm_gbs"])
+        if v > 0:
+            return v, "measured"
+    except (OSError, ValueError, KeyError, TypeError):
+        pass
     return 6650.0, "fallback"
 
 
