@@ -86,3 +86,25 @@ def test_reference_arm_json_line():
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "link-upd/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
+
+
+def test_clock_summary_parses_nvidia_smi_lines():
+    """The clock sampler's reading of nvidia-smi's csv,noheader,nounits lines: median SM clock,
+    max clock, the reasons seen active at any sample; malformed samples are skipped."""
+    import tempfile
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    c = bench.Clocks.__new__(bench.Clocks)
+    c.proc = object()
+    c.f = tempfile.TemporaryFile(mode="w+")
+    c.f.write("0, 1950, 1965, 980.12, 0x0000000000000004, Not Active, Not Active, Not Active, Active\n"
+              "0, [N/A], 1965, 990.00, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active\n"
+              "0, 1890, 1965, 1001.50, 0x0000000000000008, Active, Not Active, Not Active, Not Active\n"
+              "garbage\n")
+    s = c.summary()
+    assert s == {"sm_mhz": 1920.0, "sm_max_mhz": 1965.0, "reasons": ["hw_slowdown", "sw_power_cap"],
+                 "samples": 2}
+    c.proc = None
+    assert c.summary()["reasons"] == ["nvidia-smi unavailable"]
