@@ -138,3 +138,35 @@ def test_checked_library_exports_every_declared_symbol(qcb):
     assert not missing, missing
     lib.qcb_version.restype = ctypes.c_char_p
     assert b"checked" in lib.qcb_version() and b"checked" not in qcb.lib().qcb_version()
+
+
+def test_argument_validation_needs_no_device(qcb):
+    """Invalid arguments are refused on the host with QCB_EINVAL before any device call, so this
+    runs without a GPU: odd, too small and too large extents, unknown precision or storage, a
+    non-positive coupling, null handles and pointers."""
+    import ctypes as C
+
+    lib = qcb.load_library()
+    h = C.c_void_p()
+    L4 = lambda *v: (C.c_int * 4)(*v)  # noqa: E731
+    dummy = C.c_void_p(256)
+    for L, prec, store in [((3, 4, 4, 4), 64, 0), ((4, 4, 4, 0), 64, 0), ((2048, 2048, 2048, 2), 64, 0),
+                           ((4, 4, 4, 4), 16, 0), ((4, 4, 4, 4), 64, 2)]:
+        assert lib.qcb_field_create(L4(*L), prec, store, C.byref(h)) == -1, (L, prec, store)
+    assert lib.qcb_field_create(L4(4, 4, 4, 4), 64, 0, None) == -1
+    seeds = (C.c_uint64 * 2)(1, 2)
+    assert lib.qcb_batch_create(2, (C.c_int * 8)(4, 4, 4, 4, 4, 4, 4, 5), (C.c_double * 2)(6.0, 6.0), seeds,
+                                64, 0, C.byref(h)) == -1
+    assert b"lattice 1" in lib.qcb_last_error()
+    assert lib.qcb_batch_create(2, (C.c_int * 8)(*([4] * 8)), (C.c_double * 2)(6.0, 0.0), seeds, 64, 0,
+                                C.byref(h)) == -1
+    assert b"beta" in lib.qcb_last_error()
+    assert lib.qcb_batch_create(0, None, None, None, 64, 0, C.byref(h)) == -1
+    assert lib.qcb_serve_create(1 << 30, 64, 0, 0, 0, C.byref(h)) == -1  # n_rk < 1
+    assert lib.qcb_serve_submit(None, 1, L4(4, 4, 4, 4), dummy, 0.02, 5) == -1
+    assert lib.qcb_plaquette_noalloc(L4(4, 4, 4, 3), dummy, dummy, None) == -1
+    for call in (lambda: lib.qcb_hb_sweep(None, 6.0, 1, 1, 0), lambda: lib.qcb_plaquette(None, None),
+                 lambda: lib.qcb_field_prefetch_aos(None, None), lambda: lib.qcb_field_commit_prefetch(None),
+                 lambda: lib.qcb_debug_probe_link(None, 0, 0, 0), lambda: lib.qcb_ildg_write_ex(None, b"x", 0),
+                 lambda: lib.qcb_ildg_read(None, b"x")):
+        assert call() == -1
