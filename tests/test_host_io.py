@@ -46,3 +46,17 @@ def test_defaults_and_missing_file(dump, tmp_path):
     assert (p["N_switch_eo"], p["N_shift"], p["N_therm"], p["N_rk_steps"]) == ("3", "2", "100", "40")
     rc, _ = parse(dump, str(tmp_path / "missing.txt"))
     assert rc == 3
+
+
+def test_reference_signature_program_compiles_and_links(tmp_path):
+    """A C++ program written against the reference's declarations (GaugeField, GeometryCB,
+    mpi::heatbathcb::samples, GradientFlow, mpi::observables, ILDG, shift) compiles against
+    host/src/ and links against libqcb_compat.a and libqcb.so: the drop-in boundary holds at build
+    time, with no GPU.  Running it is the GPU test tests/test_gpu_compat.py."""
+    pkg = os.path.join(ROOT, "ecmc-qcb_b200")
+    exe = str(tmp_path / "compat_check")
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-I" + os.path.join(pkg, "host", "src"),
+                        os.path.join(ROOT, "tests", "cpp", "compat_check.cpp"), os.path.join(pkg, "libqcb_compat.a"),
+                        "-L" + pkg, "-lqcb", "-Wl,-rpath," + pkg, "-o", exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert os.path.exists(exe)
