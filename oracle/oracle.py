@@ -2,9 +2,9 @@
 
 The oracle checks the CUDA product: only tests/, __graft_entry__.smoke() and the
 cpu_baseline / reference legs of bench.py import it.  The product
-(ecmc-qcb_b200/) never does.  Parity is unpinned by reference fixtures (the
-reference ships none and cannot be compiled in this image); the restatement
-is pinned to analytic known answers in tests/test_oracle.py.
+(ecmc-qcb_b200/) never does.  The restatement is pinned to the reference's own
+hot-path code compiled unchanged into oracle/_ref (ref.py, tests/test_ref_pin.py)
+and to analytic known answers (tests/test_oracle.py).
 
 Fields are numpy complex128 arrays of shape (V, 4, 3, 3) in the AoS/ILDG
 order: site index lexicographic with x fastest, then mu, then the row-major

@@ -12,8 +12,9 @@
 //     std::mt19937_64 per thread (src/bin/gauge_hb_cb.cpp:31-36), and our own
 //     Haar SU(3) generator for hot starts (the reference's Householder-QR
 //     generator, src/su3/utils.cpp:13-30, needs Eigen's QR).
-// Parity: unpinned by reference fixtures (the reference ships none and cannot
-// be compiled here); pinned to analytic known answers by tests/test_oracle.py.
+// Parity: pinned to the reference's own hot-path sources, compiled unchanged into
+// oracle/_ref/libqcb_ref.so (tests/test_ref_pin.py), and to analytic known answers
+// (tests/test_oracle.py).
 #include "qcb_oracle.h"
 
 #include <omp.h>

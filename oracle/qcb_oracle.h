@@ -6,13 +6,16 @@
  * cpu_baseline / --impl reference legs of bench.py may load it.  Nothing in
  * the product links or calls it.
  *
- * Parity status: UNPINNED by reference fixtures.  The reference
- * (yacobozdalkiran/ECMC-QCB) ships no tests, no golden vectors and no sample
- * configuration, and it cannot be compiled here (it needs Eigen 3.4.0, MPI
- * and c-lime, none of which exist in this image).  This file restates the
- * reference's algorithms operation for operation and is pinned instead to
- * analytic known answers (cold start, abelian plaquette, exp of diagonal
- * su(3) elements, Philox known-answer vector) by tests/test_oracle.py.
+ * Parity status: PINNED to the reference's own code.  The reference ships no tests, golden
+ * vectors or sample configuration, and its CMake build fetches Eigen and c-lime over the network.
+ * Its hot-path sources are instead compiled unchanged (oracle/Makefile `ref`) against
+ * project-written stand-ins for the Eigen API subset they use, a one-rank MPI and a Philox replay
+ * engine in place of std::mt19937_64, into oracle/_ref/libqcb_ref.so.  tests/test_ref_pin.py
+ * holds this restatement to that library (staples, plaquette, clover Q/E, RK3 steps, flow
+ * measurement, heatbath sets and chained sweeps, shift, projection) and to fixtures it wrote
+ * (tests/golden/ref_4444.npz), within 1e-12; they agree bit for bit except for the last bit of
+ * the order-dependent global sums.  Analytic known answers (cold start, abelian plaquette, exp of
+ * diagonal su(3) elements, Philox known-answer vectors) are checked in tests/test_oracle.py.
  *
  * Layout used by every function ("AoS"): a periodic L0*L1*L2*L3 lattice with
  * no halo, sites in lexicographic order with x fastest and t slowest, 4

@@ -34,6 +34,15 @@ def load_oracle():
     return oracle
 
 
+def load_reference():
+    """The reference's own hot-path code (oracle/_ref/libqcb_ref.so), or None when it is not built."""
+    if ORACLE_DIR not in sys.path:
+        sys.path.insert(0, ORACLE_DIR)
+    import ref  # noqa: E402
+
+    return ref if (ref.available() or ref.build()) else None
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); calls libqcb.so")
     config.addinivalue_line("markers", "slow: long CPU test")
@@ -47,6 +56,14 @@ def qcb():
 @pytest.fixture(scope="session")
 def orc():
     return load_oracle()
+
+
+@pytest.fixture(scope="session")
+def refc():
+    r = load_reference()
+    if r is None:
+        pytest.skip("oracle/_ref/libqcb_ref.so is not built (make -C oracle ref needs the reference tree)")
+    return r
 
 
 @pytest.fixture(scope="session")

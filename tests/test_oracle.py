@@ -1,8 +1,8 @@
 """The CPU oracle against the golden fixtures and analytic known answers (no GPU).
 
-Parity with the reference is unpinned by reference fixtures (the reference ships none and
-cannot be compiled here); these tests pin the oracle to an independent restatement
-(tests/golden/make_golden.py) and to closed-form results.
+These tests pin the oracle to an independent numpy restatement (tests/golden/make_golden.py)
+and to closed-form results.  Its pin to the reference's own compiled hot-path code is in
+tests/test_ref_pin.py.
 """
 import math
 import os
