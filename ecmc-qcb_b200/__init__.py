@@ -68,6 +68,7 @@ def exported_symbols():
         "qcb_random_shift": (i, [_vp, u64, u64, i, _i4]),
         "qcb_hb_subsweep": (i, [_vp, d, i, u64, u32, i, i]),
         "qcb_hb_sweep": (i, [_vp, d, i, u64, u32]),
+        "qcb_hb_link": (i, [_vp, C.c_int64, i, d, i, u64, u32, _vp]),
         "qcb_plaquette": (i, [_vp, pd]),
         "qcb_clover_qe": (i, [_vp, pd, pd]),
         "qcb_flow_create": (i, [_vp, d, i, i, C.POINTER(_vp)]),
@@ -255,6 +256,13 @@ class GaugeField:
 
     def hb_sweep(self, beta, n_hits, seed, sweep) -> None:
         _check(lib().qcb_hb_sweep(self.h, float(beta), int(n_hits), int(seed), int(sweep)))
+
+    def hb_link(self, site, mu, beta, n_hits, seed, sweep) -> np.ndarray:
+        """n_hits hits of one link (lexicographic site index); returns the link's staple (3x3)."""
+        A = np.empty((3, 3), dtype=np.complex128)
+        _check(lib().qcb_hb_link(self.h, int(site), int(mu), float(beta), int(n_hits), int(seed), int(sweep),
+                                 A.ctypes.data))
+        return A
 
     # -- observables
     def plaquette(self) -> float:

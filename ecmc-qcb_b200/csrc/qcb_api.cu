@@ -203,15 +203,7 @@ int flow_step(qcb_flow_s* fl) {
     return QCB_OK;
 }
 
-bool valid_L(const int L[4]) {
-    if (!L) return false;
-    int64_t V = 1;
-    for (int d = 0; d < 4; d++) {
-        if (L[d] < 2 || (L[d] & 1)) return false;
-        V *= L[d];
-    }
-    return V <= ((int64_t)1 << 30);
-}
+bool valid_L(const int L[4]) { return L && lattice_ok(L); }
 
 int field_new(const int L[4], int prec, int store, cudaStream_t stream, qcb_field_s** out) {
     if (!out) return fail(QCB_EINVAL, "null output handle");
@@ -517,13 +509,23 @@ int qcb_field_copy(qcb_field dst, qcb_field src) {
     if (dst->fmt == src->fmt) {
         CK(cudaMemcpyAsync(dst->links, src->links, link_bytes(dst->fmt, dst->g.Vh), cudaMemcpyDeviceToDevice,
                            dst->stream));
-        return QCB_OK;
+    } else {
+        RET(staging_acquire(dst));
+        RET(launch(dst, QCB_K_OTHER,
+                   [&] { return fmt_ops(src->fmt).soa_to_aos(src->g, src->links, dst->staging, 0, dst->stream); }));
+        RET(upload_from_staging(dst, 0));
+        RET(staging_release(dst));
     }
-    RET(staging_acquire(dst));
-    RET(launch(dst, QCB_K_OTHER,
-               [&] { return fmt_ops(src->fmt).soa_to_aos(src->g, src->links, dst->staging, 0, dst->stream); }));
-    RET(upload_from_staging(dst, 0));
-    return staging_release(dst);
+    // src's later work (a heatbath, an upload) must not overwrite src's links while dst's stream is
+    // still reading them: src's stream waits for the end of the copy.
+    if (dst->stream != src->stream) {
+        cudaEvent_t ev;
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(ev, dst->stream));
+        CK(cudaStreamWaitEvent(src->stream, ev, 0));
+        cudaEventDestroy(ev);
+    }
+    return QCB_OK;
 }
 
 int qcb_cold_start(qcb_field f) {
@@ -593,6 +595,28 @@ int qcb_hb_subsweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_
         return fmt_ops(f->fmt).hb1(f->g, f->links, parity, mu, -0.75 / beta, n_hits, seed, sweep, rep, f->d_err,
                                    f->stream);
     });
+}
+
+int qcb_hb_link(qcb_field f, int64_t site, int mu, double beta, int n_hits, uint64_t seed, uint32_t sweep,
+                double* A_out) {
+    if (!f) return fail(QCB_EINVAL, "null field");
+    if (site < 0 || site >= f->g.V || mu < 0 || mu > 3 || n_hits < 0 || !(beta > 0.0))
+        return fail(QCB_EINVAL, "heatbath link: site in [0, V), mu in 0..3, n_hits >= 0, beta > 0");
+    int64_t r = site;
+    int par = 0;
+    for (int d = 0; d < 4; d++) {
+        par += (int)(r % f->L[d]);
+        r /= f->L[d];
+    }
+    par &= 1;
+    const int rep = needs_reproject(f->prec, f->store);
+    RET(launch(f, QCB_K_HB, [&] {
+        return fmt_ops(f->fmt).hb_one(f->g, f->links, par, (int)(site >> 1), mu, -0.75 / beta, n_hits, seed, sweep,
+                                      rep, f->d_err, (double2*)f->d_res, f->stream);
+    }));
+    RET(read_results(f, 18));
+    if (A_out) memcpy(A_out, f->h_res, 18 * sizeof(double));
+    return check_err_flag(f);
 }
 
 int qcb_hb_sweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_t sweep) {

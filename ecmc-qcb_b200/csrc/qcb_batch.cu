@@ -180,13 +180,8 @@ int qcb_batch_create(int n, const int* L, const double* beta, const uint64_t* se
     if (prec != QCB_PREC_F64 && prec != QCB_PREC_F32) return fail(QCB_EINVAL, "prec must be 64 or 32");
     if (store != QCB_STORE_18 && store != QCB_STORE_12) return fail(QCB_EINVAL, "store must be 0 or 1");
     for (int i = 0; i < n; i++) {
-        int64_t V = 1;
-        for (int d = 0; d < 4; d++) {
-            const int l = L[4 * i + d];
-            if (l < 2 || (l & 1)) return fail(QCB_EINVAL, "batch lattice %d: extents must be even and >= 2", i);
-            V *= l;
-        }
-        if (V > ((int64_t)1 << 30)) return fail(QCB_EINVAL, "batch lattice %d: volume exceeds 2^30", i);
+        if (!lattice_ok(L + 4 * i))
+            return fail(QCB_EINVAL, "batch lattice %d: extents must be even, >= 2, volume <= 2^30", i);
         if (!(beta[i] > 0.0)) return fail(QCB_EINVAL, "batch lattice %d: beta must be > 0", i);
     }
     qcb_batch_s* b = new (std::nothrow) qcb_batch_s();

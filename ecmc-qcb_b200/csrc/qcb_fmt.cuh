@@ -90,6 +90,17 @@ struct FmtImpl {
             default: return hb1_mu<3>(g, links, par, c_alpha, n_hits, seed, sweep, rep, err, s);
         }
     }
+    static cudaError_t hb_one(const Geom& g, void* links, int par, int h, int mu, double c_alpha, int n_hits,
+                              uint64_t seed, uint32_t sweep, int rep, int* err, double2* a_out, cudaStream_t s) {
+        auto U = view(links, g.Vh);
+        switch (mu) {
+            case 0: k_hb_one<R, NE, 0><<<1, 1, 0, s>>>(g, U, par, h, c_alpha, n_hits, seed, sweep, rep, err, a_out); break;
+            case 1: k_hb_one<R, NE, 1><<<1, 1, 0, s>>>(g, U, par, h, c_alpha, n_hits, seed, sweep, rep, err, a_out); break;
+            case 2: k_hb_one<R, NE, 2><<<1, 1, 0, s>>>(g, U, par, h, c_alpha, n_hits, seed, sweep, rep, err, a_out); break;
+            default: k_hb_one<R, NE, 3><<<1, 1, 0, s>>>(g, U, par, h, c_alpha, n_hits, seed, sweep, rep, err, a_out); break;
+        }
+        return cudaGetLastError();
+    }
     static cudaError_t probe_link(const Geom& g, const void* links, int mu, int par, int h, double* out,
                                   cudaStream_t s) {
         k_probe_link<R, NE><<<1, 1, 0, s>>>(view(links, g.Vh), mu, par, h, out);
@@ -175,6 +186,7 @@ struct FmtImpl {
         o.plaq_tiles = &plaq_tiles;
         o.clover_tiles = &clover_tiles;
         o.hb1 = &hb1;
+        o.hb_one = &hb_one;
         o.probe_link = &probe_link;
         o.flow1 = &flow1;
         o.plaquette = &plaquette;

@@ -21,6 +21,19 @@ inline size_t tiled_sites(int64_t Vh) { return (size_t)((Vh + 31) / 32) * 32; }
 inline size_t link_bytes(int fmt, int64_t Vh) { return (size_t)8 * fmt_ne(fmt) * tiled_sites(Vh) * fmt_cbytes(fmt); }
 inline size_t alg_bytes(int fmt, int64_t Vh) { return (size_t)8 * 4 * tiled_sites(Vh) * fmt_cbytes(fmt); }
 
+// Lattice extents every entry point accepts: even, >= 2, at most 2^30 sites.  The running volume
+// is checked after each factor (and every factor is at most 2^30), so no product overflows.
+inline bool lattice_ok(const int* L, int64_t* V_out = nullptr) {
+    int64_t V = 1;
+    for (int d = 0; d < 4; d++) {
+        if (L[d] < 2 || (L[d] & 1) || L[d] > (1 << 30)) return false;
+        V *= L[d];
+        if (V > ((int64_t)1 << 30)) return false;
+    }
+    if (V_out) *V_out = V;
+    return true;
+}
+
 int fail(int code, const char* fmt, ...);
 // Adds n to the process-wide kernel launch counter reported by qcb_launch_count().
 void note_launches(int n);

@@ -576,6 +576,23 @@ __global__ void __launch_bounds__(QCB_HB_THREADS, QCB_HB_MINB(R))
                              QCB_HB_THREADS);
 }
 
+// One link's heatbath update (the C ABI's single-link entry, qcb_hb_link; reference
+// mpi::heatbathcb::hit, src/heatbath/heatbath_mpi.cpp:10-33).  One thread: the staple A of the
+// link, formed with explicit three-row products as compute_staple forms it, goes to a_out
+// (9 double2, what hit() leaves in its SU3& argument); then n_hits hits update the link with the
+// same arithmetic and the same Philox stream as the (parity, mu) sub-sweep gives that link.
+template <typename R, int NE, int MU>
+__global__ void k_hb_one(Geom g, LinkField<R, NE> U, int par, int h, double c_alpha, int n_hits, uint64_t seed,
+                         uint32_t sweep, int reproject, int* err, double2* a_out) {
+    int c[4];
+    site_coords(g, par, (uint32_t)h, c);
+    const int lex = lex_of(g, c);
+    const M3<R> A = staple_rt<R, NE>(g, U, c, lex, par, MU);
+#pragma unroll
+    for (int k = 0; k < 9; k++) a_out[k] = make_double2((double)A.e[k].re, (double)A.e[k].im);
+    hb_link<R, NE, MU, false>(g, U, par, h, c_alpha, n_hits, seed, sweep, reproject, err, nullptr, 0);
+}
+
 // ------------------------------------------------------------------ Wilson flow
 // One fused RK3 stage (src/flow/gradient_flow.cpp:17-121) for every link (x, mu):
 //   F = proj_lie_su3(-U A)                                          compute_force

@@ -16,8 +16,12 @@
 //     before reading it, so nothing has to start at zero;
 //   * the first call on each device looks the array's device address up with
 //     cudaGetSymbolAddress (with that device current) and caches it; make that first call
-//     before any stream capture begins on the device.
+//     before any stream capture begins on the device.  The cached address belongs to the
+//     device's current context: a cudaDeviceReset (or any other teardown of the primary
+//     context) between calls is not supported, because the module may reload elsewhere.
 #include <cuda_runtime.h>
+
+#include <stdint.h>
 
 #include <mutex>
 
@@ -75,12 +79,11 @@ __global__ void k_noalloc_final(const double* partials, int nb, double norm, dou
 
 extern "C" int qcb_plaquette_noalloc(const int L[4], const double* d_links, double* d_plaq, void* stream) {
     if (!L || !d_links || !d_plaq) return fail(QCB_EINVAL, "null argument");
-    int64_t V = 1;
-    for (int d = 0; d < 4; d++) {
-        if (L[d] < 2 || (L[d] & 1)) return fail(QCB_EINVAL, "lattice extents must be even and >= 2");
-        V *= L[d];
-    }
-    if (V > ((int64_t)1 << 30)) return fail(QCB_EINVAL, "lattice volume %lld exceeds 2^30 sites", (long long)V);
+    int64_t V = 0;
+    if (!lattice_ok(L, &V)) return fail(QCB_EINVAL, "lattice extents must be even, >= 2, volume <= 2^30 sites");
+    // the kernel reads the links as 16-byte (re, im) pairs and writes one double
+    if (((uintptr_t)d_links & 15u) != 0) return fail(QCB_EINVAL, "d_links must be 16-byte aligned");
+    if (((uintptr_t)d_plaq & 7u) != 0) return fail(QCB_EINVAL, "d_plaq must be 8-byte aligned");
     const Geom g = make_geom(L);
     const int64_t need = (g.Vh + 255) / 256;
     const unsigned nbx = (unsigned)(need < 148 * 8 ? need : 148 * 8);

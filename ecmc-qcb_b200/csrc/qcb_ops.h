@@ -32,6 +32,8 @@ struct FmtOps {
     // ---- single-lattice kernels
     cudaError_t (*hb1)(const Geom& g, void* links, int par, int mu, double c_alpha, int n_hits, uint64_t seed,
                        uint32_t sweep, int reproject, int* err, cudaStream_t s);
+    cudaError_t (*hb_one)(const Geom& g, void* links, int par, int h, int mu, double c_alpha, int n_hits,
+                          uint64_t seed, uint32_t sweep, int reproject, int* err, double2* a_out, cudaStream_t s);
     cudaError_t (*probe_link)(const Geom& g, const void* links, int mu, int par, int h, double* out,
                               cudaStream_t s);
     cudaError_t (*flow1)(const Geom& g, const void* win, void* wout, void* z, double eps, int stage, int reproject,

@@ -437,12 +437,8 @@ double qcb_serve_now(qcb_server s) { return s ? s->now() : 0.0; }
 
 int qcb_serve_submit(qcb_server s, uint64_t id, const int L[4], const double* links, double eps, int n_steps) {
     if (!s || !L || !links || !(eps > 0.0) || n_steps < 1) return fail(QCB_EINVAL, "serve submit: invalid argument");
-    int64_t V = 1;
-    for (int d = 0; d < 4; d++) {
-        if (L[d] < 2 || (L[d] & 1)) return fail(QCB_EINVAL, "serve submit: extents must be even and >= 2");
-        V *= L[d];
-    }
-    if (V > ((int64_t)1 << 30)) return fail(QCB_EINVAL, "serve submit: volume exceeds 2^30");
+    int64_t V = 0;
+    if (!lattice_ok(L, &V)) return fail(QCB_EINVAL, "serve submit: extents must be even, >= 2, volume <= 2^30");
     Request* r = new (std::nothrow) Request();
     if (!r) return fail(QCB_ENOMEM, "host allocation");
     r->id = id;

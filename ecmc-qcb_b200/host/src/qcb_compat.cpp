@@ -174,6 +174,18 @@ void GaugeField::compute_staple(const GeometryCB& geo, size_t site, int mu, SU3&
 
 // ====================================================================== heatbath
 namespace mpi::heatbathcb {
+void hit(GaugeField& field, const GeometryCB& geo, size_t site, int mu, double beta, SU3& A, std::mt19937_64& rng) {
+    int c[4];
+    geo.coords(site, c);
+    int64_t lex = 0;
+    for (int d = 3; d >= 0; d--) lex = lex * geo.L_int + (((c[d] - 1) % geo.L_int) + geo.L_int) % geo.L_int;
+    const uint64_t key = rng();
+    double a[18];
+    qcb_check(qcb_hb_link(field.device(), lex, mu, beta, 1, key, 0u, a), "heatbath hit");
+    for (int k = 0; k < 9; k++) A.m[k] = Complex(a[2 * k], a[2 * k + 1]);
+    field.mark_device_modified();
+}
+
 void sweep(GaugeField& field, const GeometryCB&, double beta, int N_hits, std::vector<std::mt19937_64>& rng,
            site_parity update_parity) {
     if (!field.hb_seeded) {

@@ -111,6 +111,14 @@ int qcb_random_shift(qcb_field f, uint64_t seed, uint64_t idx, int max_shift, in
  * n_hits Cabibbo-Marinari hits over the subgroups (0,1),(1,2),(0,2), with uniforms from a
  * Philox stream keyed on seed and countered on (draw, link, sweep). */
 int qcb_hb_subsweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_t sweep, int parity, int mu);
+/* mpi::heatbathcb::hit (src/heatbath/heatbath_mpi.cpp:10-33, declared heatbath_mpi.h:14) on one
+ * link: site is the lexicographic index x + L0*(y + L1*(z + L2*t)) of the periodic lattice.  The
+ * link receives n_hits Cabibbo-Marinari hits with exactly the arithmetic and the Philox stream
+ * (seed, sweep) that qcb_hb_subsweep gives it; A_out (may be NULL) receives the link's staple,
+ * 9 complex as 18 doubles, row-major -- what hit() leaves in its SU3& A argument.  Synchronises
+ * the field's stream. */
+int qcb_hb_link(qcb_field f, int64_t site, int mu, double beta, int n_hits, uint64_t seed, uint32_t sweep,
+                double* A_out);
 /* Full sweep: (parity 0, mu 0..3) then (parity 1, mu 0..3).  Replaces the pair
  * sweep(EV); sweep(OD) of mpi::heatbathcb::samples (heatbath_mpi.cpp:60-75).  FP32 fields and
  * 12-real fields are reprojected to SU(3) in FP64 after each link update. */
@@ -257,11 +265,14 @@ int qcb_serve_stats(qcb_server s, double* out);
  * d_links: FP64 links in the parity-split layout of a QCB_PREC_F64 / QCB_STORE_18 field:
  *   complex element (row r, col c) of link (x, mu) at d_links[2*(((mu*2 + p)*9 + 3r + c)*V/2 + lex(x)/2)]
  *   (+1 for the imaginary part), lex(x) = x0 + L0*(x1 + L1*(x2 + L2*x3)), p = (x0+x1+x2+x3) mod 2.
+ * d_links must be 16-byte aligned (its (re, im) pairs are read as 16-byte words) and d_plaq 8-byte
+ * aligned; other pointers are refused with QCB_EINVAL.
  * Limits: even extents >= 2, volume <= 2^30 sites.  Scratch: a fixed static device array of
  * 2*148*8 doubles (18.5 KiB) that every GPU loading the library holds until exit; all calls
  * share it and it keeps the last call's contents, so calls that overlap on the GPU race.  The
  * first call on a device looks the array's address up (cudaGetSymbolAddress) with that device
- * current; make it before any stream capture on that device. */
+ * current; make it before any stream capture on that device.  The address is kept for the life of
+ * the process, so resetting the device (cudaDeviceReset) between calls is not supported. */
 int qcb_plaquette_noalloc(const int L[4], const double* d_links, double* d_plaq, void* stream);
 
 #ifdef __cplusplus

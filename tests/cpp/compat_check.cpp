@@ -86,5 +86,16 @@ int main(int argc, char** argv) {
     int s[4] = {1, 2, 0, 3};
     mpi::shift::shift_field(field, geo, hs, topo, s);
     dump(field, geo, dir + "/shift.bin");
+
+    // one hit of link ((2,1,1,1), mu = 1) -- interior site (1,0,0,0), lexicographic index 1 -- with
+    // the reference's signature; its staple comes back in A
+    std::mt19937_64 hit_rng(11);
+    std::cout << "hit_key " << std::mt19937_64(11)() << "\n";
+    SU3 A;
+    mpi::heatbathcb::hit(field, geo, geo.index(2, 1, 1, 1), 1, 6.0, A, hit_rng);
+    std::cout << "hit_staple";
+    for (int k = 0; k < 9; k++) std::cout << " " << A.m[k].real() << " " << A.m[k].imag();
+    std::cout << "\n";
+    dump(field, geo, dir + "/hit.bin");
     return 0;
 }

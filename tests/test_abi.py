@@ -165,6 +165,16 @@ def test_argument_validation_needs_no_device(qcb):
     assert lib.qcb_serve_create(1 << 30, 64, 0, 0, 0, C.byref(h)) == -1  # n_rk < 1
     assert lib.qcb_serve_submit(None, 1, L4(4, 4, 4, 4), dummy, 0.02, 5) == -1
     assert lib.qcb_plaquette_noalloc(L4(4, 4, 4, 3), dummy, dummy, None) == -1
+    # misaligned caller pointers are refused before any device call: links must be 16-byte aligned
+    # (read as (re, im) pairs), the output 8-byte aligned
+    assert lib.qcb_plaquette_noalloc(L4(4, 4, 4, 4), C.c_void_p(256 + 8), dummy, None) == -1
+    assert b"16-byte" in lib.qcb_last_error()
+    assert lib.qcb_plaquette_noalloc(L4(4, 4, 4, 4), dummy, C.c_void_p(256 + 4), None) == -1
+    # extents whose product overflows 64 bits are refused, not wrapped
+    big = L4(65536, 65536, 65536, 65536)
+    assert lib.qcb_field_create(big, 64, 0, C.byref(h)) == -1
+    assert lib.qcb_plaquette_noalloc(big, dummy, dummy, None) == -1
+    assert lib.qcb_batch_create(1, big, (C.c_double * 1)(6.0), seeds, 64, 0, C.byref(h)) == -1
     for call in (lambda: lib.qcb_hb_sweep(None, 6.0, 1, 1, 0), lambda: lib.qcb_plaquette(None, None),
                  lambda: lib.qcb_field_prefetch_aos(None, None), lambda: lib.qcb_field_commit_prefetch(None),
                  lambda: lib.qcb_debug_probe_link(None, 0, 0, 0), lambda: lib.qcb_ildg_write_ex(None, b"x", 0),

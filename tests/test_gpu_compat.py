@@ -1,5 +1,5 @@
-"""The C++ layer with the reference's signatures (GaugeField, GeometryCB, heatbathcb::samples,
-GradientFlow, observables, ILDG, shift) against the oracle, through a compiled C++ program."""
+"""The C++ layer with the reference's signatures (GaugeField, GeometryCB, heatbathcb::hit and
+samples, GradientFlow, observables, ILDG, shift) against the oracle, through a compiled C++ program."""
 import os
 import subprocess
 
@@ -27,7 +27,7 @@ def run(tmp_path_factory, gpu):
     for line in r.stdout.splitlines():
         parts = line.split()
         if parts and parts[0] in ("hot_key", "plaq_hot", "halo_diff", "staple00", "hb_key", "hb_sweep", "plaq_hb",
-                                  "tqe", "ildg_diff", "plaq_edit"):
+                                  "tqe", "ildg_diff", "plaq_edit", "hit_key", "hit_staple"):
             out[parts[0]] = parts[1:]
     return d, out
 
@@ -74,3 +74,20 @@ def test_ildg_edit_shift(run, orc):
     S = E.copy()
     orc.shift(S, L, [1, 2, 0, 3])
     assert np.array_equal(load(d, "shift.bin"), S)
+
+
+def test_hit_with_reference_signature(run, orc):
+    """mpi::heatbathcb::hit on one link: the staple left in A and the updated link against the oracle's
+    update of that link (one hit, Philox key = the hit's draw of its std::mt19937_64, sweep 0); every
+    other link unchanged."""
+    d, out = run
+    L = (4, 4, 4, 4)
+    S = load(d, "shift.bin")
+    A = np.array([float(x) for x in out["hit_staple"]]).view(np.complex128).reshape(3, 3)
+    assert rel_err(A, orc.staple_field(S, L, 1)[1]) < 1e-12
+    W = S.copy()
+    orc.hb_subsweep(W, L, 6.0, 1, int(out["hit_key"][0]), 0, 1, 1)  # site 1 has parity 1
+    H = load(d, "hit.bin")
+    assert rel_err(H[1, 1], W[1, 1]) < 1e-12
+    H[1, 1] = S[1, 1]
+    assert np.array_equal(H, S)

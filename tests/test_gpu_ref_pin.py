@@ -1,0 +1,227 @@
+"""The CUDA path against the reference's own hot-path code, through the C ABI (FP64 builds).
+
+Three pins:
+  * tests/golden/ref_4444.npz, written by the reference's unchanged sources
+    (tests/golden/make_ref_golden.py), for both FP64 link storages;
+  * the reference library oracle/_ref/libqcb_ref.so itself on 8^4 and 16^4 lattices (where that
+    library was built and travelled with the repository);
+  * the restated oracle (itself pinned to the reference in tests/test_ref_pin.py) at the 32^4 size
+    of the FP64 benchmark configuration, where the kernels' 32-bit site arithmetic and
+    invariant-divisor indexing run at full size.
+
+Tolerance: 1e-12 relative for links, staples, plaquette and E; Q, a signed sum near zero, within
+1e-12 * max(1, sum_x |q(x)|).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "ref_4444.npz")
+STORES = [0, 1]
+
+
+@pytest.fixture(scope="module")
+def rg():
+    g = np.load(GOLDEN)
+    return {k: g[k] for k in g.files}
+
+
+def q_tol(orc, U, L):
+    q, _ = orc.clover_qe_density(U, L)
+    return TOL * max(1.0, float(np.abs(q).sum()))
+
+
+# ---------------------------------------------------------------- fixtures the reference wrote
+@pytest.mark.parametrize("store", STORES)
+def test_reference_fixture_observables_staples_flow(gpu, orc, rg, store):
+    L = tuple(int(v) for v in rg["L"])
+    U = np.ascontiguousarray(rg["U"])
+    f = gpu.GaugeField(L, 64, store)
+    f.upload(U)
+    for mu in range(4):
+        assert rel_err(f.staple(mu), rg["staple"][mu]) < TOL
+    assert abs(f.plaquette() - rg["plaq"]) < TOL * abs(rg["plaq"])
+    Q, E = f.clover_qe()
+    assert abs(Q - rg["Q"]) < q_tol(orc, U, L)
+    assert abs(E - rg["E"]) < TOL * rg["E"]
+    fl = gpu.GradientFlow(f, 0.02)
+    fl.rk3_step(1)
+    assert rel_err(fl.field.download(), rg["U_rk3"]) < TOL
+    tqe = fl.measure(f, 5, 2)
+    assert np.array_equal(tqe[:, 0], rg["tQE"][:, 0])
+    assert np.max(np.abs(tqe[:, 1] - rg["tQE"][:, 1])) < q_tol(orc, U, L)
+    assert rel_err(tqe[:, 2], rg["tQE"][:, 2]) < TOL
+
+
+def test_reference_fixture_heatbath(gpu, rg):
+    L = tuple(int(v) for v in rg["L"])
+    f = gpu.GaugeField(L, 64, 0)
+    f.upload(np.ascontiguousarray(rg["U"]))
+    f.hb_subsweep(6.0, 2, 12345, 3, 0, 1)
+    assert rel_err(f.download(), rg["U_hb_sub"]) < TOL
+    f.upload(np.ascontiguousarray(rg["U"]))
+    f.hb_sweep(6.0, 2, 12345, 3)
+    assert rel_err(f.download(), rg["U_hb_sweep"]) < TOL
+
+
+def test_reference_fixture_exp(gpu, rg):
+    for k, c in enumerate(rg["exp_coeff"]):
+        assert np.max(np.abs(gpu.exp_su3(rg["exp_in"], c) - rg["exp_out"][k])) < 1e-14
+
+
+# ---------------------------------------------------------------- the reference library, live
+def _config(orc, L, seed):
+    LL = (L,) * 4
+    U = orc.hot_start(LL, seed)
+    orc.hb_sweep(U, LL, 6.0, 2, seed + 1, 0)
+    return LL, U
+
+
+@pytest.mark.parametrize("L", [8, 16])
+def test_reference_library_observables_and_flow(gpu, orc, refc, L):
+    LL, U = _config(orc, L, 101)
+    r = refc.RefLattice(L, U)
+    f = gpu.GaugeField(LL, 64, 0)
+    f.upload(U)
+    for mu in range(4):
+        assert rel_err(f.staple(mu), r.staple_field(mu)) < TOL
+    assert abs(f.plaquette() - r.plaquette()) < TOL * abs(r.plaquette())
+    Q, E = f.clover_qe()
+    Qr, Er = r.clover_qe()
+    assert abs(Q - Qr) < q_tol(orc, U, LL)
+    assert abs(E - Er) < TOL * Er
+    fl = gpu.GradientFlow(f, 0.02)
+    want = r.flow_measure(0.02, 4, 2)
+    got = fl.measure(f, 4, 2)
+    assert np.array_equal(got[:, 0], want[:, 0])
+    assert np.max(np.abs(got[:, 1] - want[:, 1])) < q_tol(orc, U, LL)
+    assert rel_err(got[:, 2], want[:, 2]) < TOL
+    r.flow_rk3(0.02, 2)
+    fl.copy(f)
+    fl.rk3_step(2)
+    assert rel_err(fl.field.download(), r.get()) < TOL
+
+
+@pytest.mark.parametrize("L,nh", [(8, 2), (16, 1)])
+def test_reference_library_heatbath_link_by_link(gpu, orc, refc, L, nh):
+    """Every (parity, mu) set: the CUDA update and the reference's hit() on the same input and the
+    same Philox draws (the reference's std::mt19937_64 replaced by their replay), link by link."""
+    LL, U = _config(orc, L, 201)
+    r = refc.RefLattice(L)
+    f = gpu.GaugeField(LL, 64, 0)
+    for p in range(2):
+        for mu in range(4):
+            r.set(U)
+            r.hb_subsweep(6.0, nh, 31337, 9, p, mu)
+            f.upload(U)
+            f.hb_subsweep(6.0, nh, 31337, 9, p, mu)
+            assert rel_err(f.download(), r.get()) < TOL, (p, mu)
+
+
+def test_reference_library_one_sweep(gpu, orc, refc):
+    LL, U = _config(orc, 8, 301)
+    r = refc.RefLattice(8, U)
+    r.hb_sweep(6.0, 2, 5, 0)
+    f = gpu.GaugeField(LL, 64, 0)
+    f.upload(U)
+    f.hb_sweep(6.0, 2, 5, 0)
+    assert rel_err(f.download(), r.get()) < TOL
+
+
+@pytest.mark.parametrize("store", STORES)
+def test_hb_link_against_reference_hit(gpu, orc, refc, store):
+    """qcb_hb_link (the C ABI behind mpi::heatbathcb::hit) on single links: the staple it returns and
+    the updated link against the reference's hit(); the link equals what the (parity, mu) sub-sweep
+    gives it; every other link is unchanged."""
+    LL, U = _config(orc, 8, 401)
+    f = gpu.GaugeField(LL, 64, store)
+    g = gpu.GaugeField(LL, 64, store)
+    for lex, mu, nh in [(0, 0, 1), (37, 2, 2), (511, 3, 1), (4095, 1, 2)]:
+        r = refc.RefLattice(8, U)
+        A_ref = r.hb_link(lex, mu, 6.0, nh, 77, 4)
+        f.upload(U)
+        before = f.download()
+        A = f.hb_link(lex, mu, 6.0, nh, 77, 4)
+        after = f.download()
+        assert rel_err(A, A_ref) < TOL, (lex, mu)
+        assert rel_err(after[lex, mu], r.get()[lex, mu]) < TOL, (lex, mu)
+        g.upload(U)
+        par = sum((lex // 8 ** d) % 8 for d in range(4)) % 2
+        g.hb_subsweep(6.0, nh, 77, 4, par, mu)
+        assert np.array_equal(after[lex, mu], g.download()[lex, mu])
+        after[lex, mu] = before[lex, mu]
+        assert np.array_equal(after, before)
+
+
+def test_hb_link_rejects_bad_arguments(gpu):
+    f = gpu.GaugeField((4, 4, 4, 4), 64, 0)
+    for site, mu, beta in [(-1, 0, 6.0), (256, 0, 6.0), (0, 4, 6.0), (0, 0, 0.0)]:
+        with pytest.raises(gpu.QcbError) as e:
+            f.hb_link(site, mu, beta, 1, 1, 0)
+        assert e.value.code == -1
+
+
+# ---------------------------------------------------------------- 32^4, the benchmark size
+@pytest.fixture(scope="module")
+def big(orc):
+    L = (32, 32, 32, 32)
+    U = orc.hot_start(L, 7)
+    orc.hb_subsweep(U, L, 6.0, 2, 11, 0, 0, 0)  # one set updated, so the field is not a pure hot start
+    return L, U
+
+
+def test_32x4_staple_plaquette_and_clover(gpu, orc, big):
+    L, U = big
+    f = gpu.GaugeField(L, 64, 0)
+    f.upload(U)
+    assert rel_err(f.staple(2), orc.staple_field(U, L, 2)) < TOL
+    assert abs(f.plaquette() - orc.plaquette(U, L)) < TOL * abs(orc.plaquette(U, L))
+    Q, E = f.clover_qe()
+    Qo, Eo = orc.clover_qe(U, L)
+    assert abs(Q - Qo) < q_tol(orc, U, L)
+    assert abs(E - Eo) < TOL * Eo
+
+
+@pytest.mark.parametrize("parity,mu", [(1, 3), (0, 1)])
+def test_32x4_heatbath_subsweep(gpu, orc, big, parity, mu):
+    L, U = big
+    f = gpu.GaugeField(L, 64, 0)
+    f.upload(U)
+    f.hb_subsweep(6.0, 2, 7, 17, parity, mu)
+    W = U.copy()
+    orc.hb_subsweep(W, L, 6.0, 2, 7, 17, parity, mu)
+    assert rel_err(f.download(), W) < TOL
+
+
+def test_32x4_rk3_step(gpu, orc, big):
+    L, U = big
+    f = gpu.GaugeField(L, 64, 0)
+    f.upload(U)
+    fl = gpu.GradientFlow(f, 0.02)
+    fl.rk3_step(1)
+    assert rel_err(fl.field.download(), orc.flow_rk3(U, L, 0.02, 1)) < TOL
+
+
+# ---------------------------------------------------------------- stream ordering of a copy
+def test_copy_then_update_of_source(gpu, orc):
+    """qcb_field_copy(dst, src) immediately followed by a heatbath on src (each field has its own
+    stream): dst must hold src's configuration from before the update."""
+    L = (16, 16, 16, 16)
+    U = orc.hot_start(L, 5)
+    src = gpu.GaugeField(L, 64, 0)
+    src.upload(U)
+    p0 = src.plaquette()
+    for fmt in [(64, 0), (64, 1), (32, 0)]:
+        dst = gpu.GaugeField(L, *fmt)
+        dst.copy_from(src)
+        src.hb_sweep(6.0, 2, 1, 0)  # queued at once on src's stream
+        src.sync()
+        tol = 1e-12 if fmt[0] == 64 else 1e-6
+        assert abs(dst.plaquette() - p0) < tol, fmt
+        src.upload(U)

@@ -42,11 +42,16 @@ def test_noalloc_plaquette_matches_regular_entry(gpu, orc, L):
     links = torch.from_numpy(soa_fp64(U, L)).to("cuda")
     out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
-    for _ in range(2):
+    for k in range(2):
         out.fill_(float("nan"))
+        stream.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         gpu.plaquette_noalloc(L, links.data_ptr(), out.data_ptr(), stream.cuda_stream)
         stream.synchronize()
+        free_after = torch.cuda.mem_get_info()[0]
         assert abs(out.item() - ref) < TOL * abs(ref)
+        if k == 1:  # the defining property: a call after the first allocates no device memory
+            assert free_after == free_before, (free_before, free_after)
 
 
 def test_noalloc_rejects_bad_sizes(gpu):
@@ -59,4 +64,8 @@ def test_noalloc_rejects_bad_sizes(gpu):
     assert e.value.code == -1
     with pytest.raises(gpu.QcbError) as e:
         gpu.plaquette_noalloc((2048, 2048, 2048, 2), links.data_ptr(), out.data_ptr())
+    assert e.value.code == -1
+    # a view offset by one double is only 8-byte aligned: refused, never sent to the device
+    with pytest.raises(gpu.QcbError) as e:
+        gpu.plaquette_noalloc((4, 4, 4, 4), links[1:].data_ptr(), out.data_ptr())
     assert e.value.code == -1
