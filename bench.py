@@ -10,9 +10,12 @@ through the C ABI with the configuration uploaded from pinned host memory each s
 plaquette read back.  The flow part of the metric (site-steps/s of the Wilson flow over the
 configuration's 250 steps, FP64 vs FP32 18- and 12-real, the RK3 integrator alone and with clover
 Q, E and the plaquette every step, with |dQ|, dE/E and dP against FP64) is measured on the same
-configuration and reported under "flow"; each form starts from an idle GPU.  Multi-GPU runs are independent replicas (weak scaling, no collective on the
-data path).  The reference arm times the CPU restatement of the reference's heatbath on the host
-cores.
+configuration and reported under "flow"; each form starts from an idle GPU.  Multi-GPU runs are
+independent replicas (weak scaling, no collective on the data path).  The reference arm and the
+cpu_baseline leg time the reference's own heatbath code (its hit() per link, staple recomputed per
+hit), compiled unchanged into oracle/_ref/libqcb_ref.so, on all host cores, one full sweep of the
+same 32^4 configuration per step; where that library is absent they fall back to the oracle's
+restatement with the same cost structure.
 """
 from __future__ import annotations
 
@@ -196,47 +199,109 @@ def cuda_timer(qcb, field):
     return stream, torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def cpu_sample(orc, seconds: float = 12.0, threads: int = 0):
-    """Times the oracle's heatbath with the reference's cost structure (staple per hit) on the host cores."""
-    orc.set_threads(threads)
-    U = orc.hot_start(L, SEED_HOT)
-    V = U.shape[0]
+CONFIG = {"workload": "hb_fp64_32^4", "L": list(L), "beta": BETA, "n_hits": N_HITS, "start": "hot seed 7",
+          "step": "one full checkerboard sweep (8 (parity,mu) passes, every link updated once)",
+          "l2": "inputs larger than L2 (604 MB FP64 field vs 126 MB L2)"}
+
+
+class CpuHeatbath:
+    """The CPU heatbath the GPU arm is compared with, on the 32^4 configuration (hot start seed 7).
+
+    kind "reference": the reference's own mpi::heatbathcb::hit (src/heatbath/heatbath_mpi.cpp:10-33)
+    link by link, compiled unchanged into oracle/_ref/libqcb_ref.so, staple recomputed for every hit
+    as the reference does, OpenMP over the links of each (parity, mu) set on all host threads, draws
+    from the same Philox link streams as the GPU.  kind "port": the oracle's restatement with the same
+    cost structure, used only where the reference library is absent."""
+
+    def __init__(self):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        orc = load_oracle()
+        orc.set_threads(0)
+        U = orc.hot_start(L, SEED_HOT)
+        self.V = U.shape[0]
+        self.threads = orc.threads()
+        import ref
+
+        if ref.available():
+            ref.set_threads(0)
+            self.kind = "reference"
+            self.lat = ref.RefLattice(L[0], U)
+            self._sub = lambda sw, p, mu: self.lat.hb_subsweep(BETA, N_HITS, SEED_HB, sw, p, mu)
+        else:
+            self.kind = "port"
+            self.U = U
+            self._sub = lambda sw, p, mu: orc.hb_subsweep(self.U, L, BETA, N_HITS, SEED_HB, sw, p, mu, refcost=True)
+
+    def sweep(self, sw: int) -> None:
+        for p in (0, 1):
+            for mu in range(4):
+                self._sub(sw, p, mu)
+
+    def describe(self, what: str) -> str:
+        src = ("the reference's hit() compiled unchanged (oracle/_ref)" if self.kind == "reference"
+               else "the oracle's restatement of the reference's hit()")
+        return (f"{what}; each sweep 8 (parity,mu) passes of V/2 = {self.V // 2} link-updates, N_hits=2, staple "
+                f"recomputed per hit; {src}; 1 process x {self.threads} OpenMP threads")
+
+
+def cpu_sample(seconds: float = 12.0):
+    """cpu_baseline leg: full sweeps of the workload on the host cores until `seconds` have passed
+    (after one untimed sweep), with the sweep indices the reference arm uses."""
+    c = CpuHeatbath()
+    c.sweep(0)
     n, t0 = 0, time.perf_counter()
     while True:
-        orc.hb_subsweep(U, L, BETA, N_HITS, SEED_HB, 0, n % 2, (n // 2) % 4, refcost=True)
+        c.sweep(1 + n)
         n += 1
         el = time.perf_counter() - t0
         if el >= seconds:
             break
-    return {"value": n * (V // 2) / el, "unit": "link-upd/s", "cores": orc.threads(), "kind": "port",
-            "sample": f"{n} (parity,mu) sub-sweeps of 32^4 (V/2 links each, N_hits=2, staple recomputed per hit "
-                      f"as heatbath_mpi.cpp:12), {el:.1f} s, 1 process x {orc.threads()} OpenMP threads"}
+    return {"value": n * 4 * c.V / el, "unit": "link-upd/s", "cores": c.threads, "kind": c.kind,
+            "sample": c.describe(f"{n} full sweeps of 32^4 in {el:.1f} s")}
+
+
+REF_BUDGET_S = 300.0  # the reference arm's whole run stays within a few minutes
 
 
 def run_reference(args, rank: int, world: int):
+    """The reference arm: W untimed then K timed steps of the workload on the host cores.  A step is
+    one full sweep, as in the GPU arm, unless W + K full sweeps would exceed REF_BUDGET_S (judged from
+    the first warm-up sweep); then a step is one (parity, mu) pass (V/2 link-updates) and the
+    config's "step" says so."""
     if rank != 0:
         return
-    orc = load_oracle()
-    orc.set_threads(0)
-    U = orc.hot_start(L, SEED_HOT)
-    V = U.shape[0]
-    times = []
-    for i in range(args.warmup + args.steps):
+    c = CpuHeatbath()
+    t0 = time.perf_counter()
+    c.sweep(0)
+    t_sweep = time.perf_counter() - t0
+    full = (args.warmup + args.steps) * t_sweep <= REF_BUDGET_S
+    times, units = [], 0
+    for i in range(1, args.warmup + args.steps):
         t0 = time.perf_counter()
-        orc.hb_subsweep(U, L, BETA, N_HITS, SEED_HB, i, i % 2, (i // 2) % 4, refcost=True)
+        if full:
+            c.sweep(i)
+        else:
+            c._sub(i // 8, (i // 4) % 2, i % 4)
         if i >= args.warmup:
             times.append(time.perf_counter() - t0)
+            units += 4 * c.V if full else c.V // 2
+    if args.warmup == 0:  # the first sweep is the only one of a 0-warm-up run that was timed
+        times.append(t_sweep)
+        units += 4 * c.V
     tot = sum(times)
-    value = args.steps * (V // 2) / tot
-    sample = (f"each step one (parity,mu) sub-sweep of the 32^4 workload (V/2 = {V // 2} link-updates, N_hits=2, "
-              f"staple recomputed per hit); CPU restatement of the reference, 1 process x {orc.threads()} threads")
+    value = units / tot
+    cfg = dict(CONFIG)
+    cfg["parallelism"] = f"replicas x{args.gpus}"
+    if not full:
+        cfg["step"] = "one (parity,mu) pass of the sweep (V/2 link-updates): full sweeps exceed the time budget"
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "link-upd/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "hb_fp64_32^4", "L": list(L), "beta": BETA, "n_hits": N_HITS, "start": "hot seed 7"},
-        "cpu_baseline": {"value": value, "unit": "link-upd/s", "cores": orc.threads(), "kind": "port",
-                         "sample": sample},
+        "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "link-upd/s", "cores": c.threads, "kind": c.kind,
+                         "sample": c.describe(f"{args.steps} timed {'full sweeps' if full else '(parity,mu) passes'} "
+                                              f"after {args.warmup} untimed")},
         "e2e": {"value": value, "unit": "link-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -497,19 +562,25 @@ def run_serve(qcb, n_req: int, stores=(0, 1), low_rates=(4.0, 2.0), n_low: int =
                        "configs_per_s": n_req / wall, "site_steps_per_s": site_steps / wall,
                        "peak_resident": st["peak_resident"], "peak_bytes": st["peak_bytes"]}
     store = max(arms, key=lambda s_: arms[s_]["configs_per_s"])
+    # the serial FP64 arm: one field and one flow state per lattice size, allocated before the timed
+    # loop (as the server's pool is), then one request at a time from its host configuration to its
+    # results
+    serial = {}
+    for x in sorted(set(int(v) for v in sizes)):
+        fx = qcb.GaugeField((x,) * 4, 64, 0)
+        serial[x] = (fx, qcb.GradientFlow(fx, 0.02, prec=64, store=0))
     tq, lat2, busy = 0.0, [], 0.0
     time.sleep(FLOW_COOL_S)
     for i in range(n_req):
-        # one request at a time, from its host configuration to its results, as the server takes it
         t0 = time.perf_counter()
-        f = qcb.GaugeField((int(sizes[i]),) * 4, 64, 0)
+        f, fl = serial[int(sizes[i])]
         f.upload(inputs[i])
-        fl = qcb.GradientFlow(f, 0.02, prec=64, store=0)
         fl.measure(f, steps[i], 1)
         dt = time.perf_counter() - t0
         busy += dt
         tq = max(tq, arr[i]) + dt
         lat2.append(tq - arr[i])
+    for f, fl in serial.values():
         fl.close()
         f.close()
     lat2 = np.array(lat2)
@@ -716,20 +787,19 @@ def run_ours(args, rank: int, world: int, local: int):
 
     cpu = None
     if rank == 0 and args.cpu_seconds > 0:
-        orc = load_oracle()
-        cpu = cpu_sample(orc, seconds=args.cpu_seconds)
+        cpu = cpu_sample(seconds=args.cpu_seconds)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "link-upd/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "hb_fp64_32^4", "L": list(L), "beta": BETA, "n_hits": N_HITS,
-                       "start": "hot seed 7", "step": "one full checkerboard sweep (8 (parity,mu) launches)",
-                       "l2": "inputs larger than L2 (604 MB FP64 field vs 126 MB L2)",
-                       "parallelism": f"replicas x{world}"},
+            "config": dict(CONFIG, parallelism=f"replicas x{world}"),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": traffic, "kernel": "k_hb_subsweep<double,9,mu>",
+                         "frac": achieved / hbm_peak, "traffic": traffic,
+                         "traffic_source": "ncu DRAM bytes per launch of this kernel, from the committed capture "
+                                           "profiles/hb_subsweep_fp64_32x4.md (not measured in this run)",
+                         "kernel": "k_hb_subsweep<double,9,mu>",
                          "per_launch_ms": per_launch_ms, "algorithmic_bytes_per_launch": bytes_launch,
                          "peak_kind": peak_kind},
             "cpu_baseline": cpu,

@@ -68,8 +68,9 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
 
 
 def test_reference_arm_json_line():
-    """The reference arm prints one JSON line with the bench contract's keys, timing the oracle's
-    heatbath on the host cores for the same workload, metric and unit as the CUDA arm."""
+    """The reference arm prints one JSON line with the bench contract's keys, timing the reference's
+    own heatbath (oracle/_ref) on the host cores for the same workload, step, metric and unit as the
+    CUDA arm."""
     import json
     import subprocess
 
@@ -82,8 +83,13 @@ def test_reference_arm_json_line():
     assert d["impl"] == "reference" and d["unit"] == "link-upd/s" and d["value"] > 0
     assert d["steps"] == 1 and d["warmup"] == 3 and d["n_gpus"] == 1 and d["higher_is_better"] is True
     assert d["config"]["workload"] == "hb_fp64_32^4" and d["dtype"] == "f64" and d["vs_baseline"] is None
+    assert d["config"]["step"].startswith("one full checkerboard sweep") and "parallelism" in d["config"]
     cb = d["cpu_baseline"]
-    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+
+    assert cb["kind"] == ("reference" if ref.available() else "port")
+    assert cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "link-upd/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
 
