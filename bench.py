@@ -310,33 +310,51 @@ FLOW_STEPS = 250  # t = 5.0 at eps = 0.02: the flow of the 32^4 FP64 configurati
 FLOW_COOL_S = 2.0  # idle pause before each timed flow form
 
 
-def flow_block(qcb, src, prec, store, n_steps, hbm_peak, gpu_index=0, measured=True):
+def flow_flops_per_link_stage(prec: int) -> float:
+    """Algorithmic flops of one link in one fused RK3 stage, as the kernels form it (complex
+    multiply-add 8 flops, multiply 6, add 2):
+      staple   6 staples x (36 multiply-adds of the two-row products + 6 multiplies and 3 subtractions
+               rebuilding row 3 + 9 adds into A)                                    = 6 x 348 = 2088
+      force    -proj(U A) from 6 off-diagonal entries (3 multiply-adds each), 3 imaginary diagonal
+               parts and the projection                                            = 204
+      RK3      X (and Z) combinations, averaged over the three stages              = 60
+      exp      X^2 (27 multiply-adds), t and det X, the 18-step Horner recurrence, q0 + q1 X + q2 X^2
+                                                                                   = 542
+      update   exp(X) W, full product (27 multiply-adds)                           = 216
+      reproject (FP32 links) column Gram-Schmidt in FP64                           = 100"""
+    return 2088 + 204 + 60 + 542 + 216 + (100 if prec == 32 else 0)
+
+
+def flow_block(qcb, src, prec, store, n_steps, hbm_peak, fma_peak, gpu_index=0, measured=True):
     """One flow form on the configuration `src`, timed with CUDA events on the flow's stream.
 
     Every form starts from the same state: an idle pause of FLOW_COOL_S first, because under the
     1 kW power cap a form timed right after another inherits its power draw (a stage runs 10-20%
     slower for a few hundred ms after a sustained FP64 flow).  Then
-      (a) n_steps RK3 steps after 3 warm-up steps: site-steps/s of the integrator and the mean
-          stage-kernel duration (per-launch events, for the roofline);
-      (b) if `measured`, the configuration's measured flow: the copy of `src`, n_steps RK3 steps
+      (a) n_steps RK3 steps after 3 warm-up steps, replayed as CUDA graphs: site-steps/s of the
+          integrator;
+      (b) 20 more steps with per-launch event timing (plain launches): the mean stage-kernel
+          duration, for the HBM roofline and the pipe fraction;
+      (c) if `measured`, the configuration's measured flow: the copy of `src`, n_steps RK3 steps
           and clover Q, E and the plaquette at every one of the n_steps + 1 times
           (qcb_flow_measure), after the same idle pause.
-    SM clocks and throttle reasons are sampled over both."""
+    SM clocks and throttle reasons are sampled over all three."""
     V = src.V
     time.sleep(FLOW_COOL_S)
     fl = qcb.GradientFlow(src, 0.02, prec=prec, store=store)
     f = fl.field
     stream, e0, e1 = cuda_timer(qcb, f)
     with Clocks(gpu_index) as clk:
-        fl.rk3_step(3)
+        fl.rk3_step(4)
         f.sync()
-        f.timing(True)
-        f.timing_reset()
         e0.record(stream)
         fl.rk3_step(n_steps)
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1)
+        f.timing(True)
+        f.timing_reset()
+        fl.rk3_step(20)
         nl, kms = f.timing_read(qcb.K_FLOW)
         f.timing(False)
         ms_meas = None
@@ -349,12 +367,18 @@ def flow_block(qcb, src, prec, store, n_steps, hbm_peak, gpu_index=0, measured=T
             ms_meas = e0.elapsed_time(e1)
     s_u = (S_U12 if store == 1 else S_U)[prec]
     bytes_stage = V * 4 * (2 * s_u) + V * 4 * S_Z[prec] * (4 / 3)  # per stage: read+write U, Z traffic averaged
-    achieved = bytes_stage / (kms / nl * 1e-3) / 1e9
+    stage_ms = kms / nl
+    achieved = bytes_stage / (stage_ms * 1e-3) / 1e9
+    flops_stage = 4 * V * flow_flops_per_link_stage(prec)
+    tflops = flops_stage / (stage_ms * 1e-3) / 1e12
     fl.close()
     out = {"site_steps_per_s": V * n_steps / (ms * 1e-3), "rk3_steps": n_steps, "ms_per_rk3": ms / n_steps,
-           "stage_kernel_ms": kms / nl,
+           "launch": "CUDA graph replays (two RK3 steps each)", "stage_kernel_ms": stage_ms,
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                         "frac": achieved / hbm_peak},
+           "pipe": {"bound": f"fp{prec}", "achieved": tflops, "peak": fma_peak[prec], "unit": "TFLOP/s",
+                    "frac": tflops / fma_peak[prec], "flops_per_site_step": 12 * flow_flops_per_link_stage(prec),
+                    "peak_kind": "measured FMA rate (qcb_diag_fma_rate)"},
            "clocks": clk.summary()}
     if ms_meas is not None:
         out["measured_flow"] = {"rk3_steps": n_steps, "measurements": n_steps + 1,
@@ -673,8 +697,9 @@ def run_ours(args, rank: int, world: int, local: int):
     if args.only == "flow":
         for i in range(args.warmup):
             f.hb_sweep(BETA, N_HITS, SEED_HB, i)
+        fma_peak = {64: qcb.fma_rate(64) / 1e12, 32: qcb.fma_rate(32) / 1e12}
         for prec, store in ((64, 0), (32, 0), (32, 1)):
-            flow_block(qcb, f, prec, store, args.steps, hbm_peak, local, measured=False)
+            flow_block(qcb, f, prec, store, args.steps, hbm_peak, fma_peak, local, measured=False)
         f.close()
         return
 
@@ -751,10 +776,11 @@ def run_ours(args, rank: int, world: int, local: int):
     del U_host
 
     # ---------------- flow: FP64 vs FP32 (18 and 12 reals) on the heatbath configuration
-    flow = {}
-    flow["fp64"] = flow_block(qcb, f, 64, 0, FLOW_STEPS, hbm_peak, local)
-    flow["fp32_18"] = flow_block(qcb, f, 32, 0, FLOW_STEPS, hbm_peak, local)
-    flow["fp32_12"] = flow_block(qcb, f, 32, 1, FLOW_STEPS, hbm_peak, local)
+    fma_peak = {64: qcb.fma_rate(64) / 1e12, 32: qcb.fma_rate(32) / 1e12}
+    flow = {"fma_peak_tflops": fma_peak}
+    flow["fp64"] = flow_block(qcb, f, 64, 0, FLOW_STEPS, hbm_peak, fma_peak, local)
+    flow["fp32_18"] = flow_block(qcb, f, 32, 0, FLOW_STEPS, hbm_peak, fma_peak, local)
+    flow["fp32_12"] = flow_block(qcb, f, 32, 1, FLOW_STEPS, hbm_peak, fma_peak, local)
     acc = flow_accuracy(qcb, f, 40)
     for k in ("fp32_18", "fp32_12"):
         flow[k].update(acc[k])

@@ -92,6 +92,7 @@ def exported_symbols():
         "qcb_diag_staple": (i, [_vp, i, _vp]),
         "qcb_diag_exp_su3": (i, [_vp, i, d, i, _vp]),
         "qcb_diag_philox": (i, [C.POINTER(u32), C.POINTER(u32), i, C.POINTER(u32)]),
+        "qcb_diag_fma_rate": (i, [i, pd]),
         "qcb_plaquette_noalloc": (i, [_i4, _vp, _vp, _vp]),
         "qcb_batch_create": (i, [i, C.POINTER(C.c_int), pd, C.POINTER(u64), i, i, C.POINTER(_vp)]),
         "qcb_batch_destroy": (i, [_vp]),
@@ -109,6 +110,7 @@ def exported_symbols():
         "qcb_serve_create": (i, [sz, i, i, i, i, C.POINTER(_vp)]),
         "qcb_serve_destroy": (i, [_vp]),
         "qcb_serve_now": (d, [_vp]),
+        "qcb_serve_set_option": (i, [_vp, i, i]),
         "qcb_serve_submit": (i, [_vp, u64, _i4, _vp, d, i]),
         "qcb_serve_poll": (i, [_vp, C.POINTER(u64), pd, i, pi, pd]),
         "qcb_serve_wait": (i, [_vp, d]),
@@ -401,6 +403,10 @@ class Server:
     def now(self) -> float:
         return lib().qcb_serve_now(self.h)
 
+    def set_graphs(self, on: bool) -> None:
+        """Replay the small requests' shared launches from CUDA graphs while the resident set is unchanged."""
+        _check(lib().qcb_serve_set_option(self.h, 1, 1 if on else 0))
+
     def submit(self, rid: int, L, U: np.ndarray, eps: float, n_steps: int) -> None:
         U = np.ascontiguousarray(U, dtype=np.complex128)
         _check(lib().qcb_serve_submit(self.h, int(rid), _i4(*[int(v) for v in L]), U.ctypes.data, float(eps),
@@ -505,6 +511,13 @@ def exp_su3(Z: np.ndarray, coeff: float, prec: int = PREC_F64) -> np.ndarray:
     out = np.empty_like(z)
     _check(lib().qcb_diag_exp_su3(z.ctypes.data, z.shape[0], float(coeff), int(prec), out.ctypes.data))
     return out
+
+
+def fma_rate(prec: int = PREC_F64) -> float:
+    """Measured FMA throughput of the current device, FLOP/s (FP64 or FP32)."""
+    r = C.c_double()
+    _check(lib().qcb_diag_fma_rate(int(prec), C.byref(r)))
+    return r.value
 
 
 def philox(ctr, key, n: int = 1) -> np.ndarray:

@@ -207,6 +207,111 @@ int flow_step(qcb_flow_s* fl) {
     return QCB_OK;
 }
 
+// ------------------------------------------------------------------ flow step graphs
+// Without per-launch timing, the flow's repeated launch sequences are captured once as CUDA graphs
+// and replayed: two RK3 steps (six stage launches; the ping-pong buffers are back in place after
+// them), and one measurement block of qcb_flow_measure (clover pass into a fixed slot, the row
+// scatter, then n_rk RK3 steps).  Replays launch the same kernels with the same arguments as the
+// plain launches, so results are identical bit for bit.
+constexpr int kMeasSlot = 32;  // d_res offset of the measurement slot (q, e, plaquette sums)
+
+int meas_block(qcb_flow_s* fl, int n_rk);
+__global__ void k_meas_scatter(const double* slot, double* meas, int* counter);
+// Graphs need a capturable stream: not the legacy default stream, and no per-launch timing events.
+bool graphs_ok(const qcb_field_s* f) { return !f->timing && f->stream != nullptr; }
+
+int flow_graph_body(qcb_flow_s* fl, int kind, int n_rk) {
+    if (kind == 1) {
+        RET(flow_step(fl));
+        return flow_step(fl);
+    }
+    return meas_block(fl, n_rk);
+}
+
+// Runs the body of graph `kind` once: replays a cached graph captured from the same buffers, or
+// captures one (the capture moves the host's ping-pong pointers as the body does; the graph is then
+// launched once to do the work).
+int flow_graph_run(qcb_flow_s* fl, int kind, int n_rk) {
+    qcb_field_s* f = fl->fld;
+    const void* links0 = f->links;
+    FlowGraph* hit = nullptr;
+    for (auto& g : fl->graphs)
+        if (g.exec && g.kind == kind && g.n_rk == n_rk && g.links == links0 && g.partials == f->partials &&
+            g.meas == fl->d_meas)
+            hit = &g;
+    if (!hit) {
+        FlowGraph* slot = &fl->graphs[0];
+        for (auto& g : fl->graphs)
+            if (!g.exec || g.last_use < slot->last_use) slot = &g;
+        if (slot->exec) cudaGraphExecDestroy(slot->exec);
+        *slot = FlowGraph{};
+        const uint64_t n0 = g_launches.load();
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(f->stream, cudaStreamCaptureModeThreadLocal));
+        int r = flow_graph_body(fl, kind, n_rk);
+        const cudaError_t e = cudaStreamEndCapture(f->stream, &graph);
+        const int kernels = (int)(g_launches.load() - n0);
+        g_launches.fetch_sub((uint64_t)kernels);  // counted when a replay runs them
+        if (r != QCB_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return r;
+        }
+        if (e != cudaSuccess) return fail(QCB_ECUDA, "flow graph capture: %s", cudaGetErrorString(e));
+        const cudaError_t ei = cudaGraphInstantiate(&slot->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) {
+            slot->exec = nullptr;
+            return fail(QCB_ECUDA, "flow graph instantiate: %s", cudaGetErrorString(ei));
+        }
+        slot->kind = kind;
+        slot->n_rk = n_rk;
+        slot->kernels = kernels;
+        slot->links = links0;
+        slot->partials = f->partials;
+        slot->meas = fl->d_meas;
+        hit = slot;
+        // the capture left the host pointers where the body leaves them; the replay below is the
+        // body's one execution, from the buffers it was captured from
+        if (f->links != links0) {
+            void* t = f->links;
+            f->links = f->alt;
+            f->alt = t;
+        }
+    }
+    hit->last_use = ++fl->graph_clock;
+    CK(cudaGraphLaunch(hit->exec, f->stream));
+    g_launches.fetch_add((uint64_t)hit->kernels);
+    // the body swaps the ping-pong buffers once per RK3 step
+    const int steps = kind == 1 ? 2 : n_rk;
+    if (steps & 1) {
+        void* t = f->links;
+        f->links = f->alt;
+        f->alt = t;
+    }
+    return QCB_OK;
+}
+
+// One measurement of the flowed field -- clover pass (q, e and the plaquette sum) into the fixed
+// slot, copied to the next row of the measurement buffer -- followed by n_rk RK3 steps.
+int meas_block(qcb_flow_s* fl, int n_rk) {
+    qcb_field_s* f = fl->fld;
+    double* slot = f->d_res + kMeasSlot;
+    RET(enq_clover(f, slot));
+    RET(launch(f, QCB_K_OTHER, [&] {
+        k_meas_scatter<<<1, 1, 0, f->stream>>>(slot, fl->d_meas, fl->d_count);
+        return cudaGetLastError();
+    }));
+    for (int k = 0; k < n_rk; k++) RET(flow_step(fl));
+    return QCB_OK;
+}
+
+void drop_flow_graphs(qcb_flow_s* fl) {
+    for (auto& g : fl->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = FlowGraph{};
+    }
+}
+
 bool valid_L(const int L[4]) { return L && lattice_ok(L); }
 
 int field_new(const int L[4], int prec, int store, cudaStream_t stream, qcb_field_s** out) {
@@ -312,6 +417,35 @@ __global__ void k_diag_exp(const double2* Z, int n, double coeff, int f32, doubl
         r = exp_su3(z);
     }
     for (int e = 0; e < 9; e++) out[i * 9 + e] = make_double2(r.e[e].re, r.e[e].im);
+}
+// Fused multiply-add throughput probe: 8 independent chains per thread, unrolled, so that the FMA
+// pipe rather than latency sets the rate; the result is kept live through a data-dependent store.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_rate(T a, T b, int iters, T* out) {
+    T x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = (T)(threadIdx.x + k) * (T)1e-3;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int k = 0; k < 8; k++) x[k] = fma(x[k], a, b);
+    }
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += x[k];
+    if (s == (T)-1) out[0] = s;  // never true for these inputs; keeps the chains
+}
+
+// Copies one measurement (q, e, plaquette sums) from the fixed slot the clover pass wrote into row
+// *counter of the measurement buffer and advances the counter (one thread; the host sizes the buffer
+// for every row it launches).
+__global__ void k_meas_scatter(const double* slot, double* meas, int* counter) {
+    const int c = *counter;
+    meas[3 * c] = slot[0];
+    meas[3 * c + 1] = slot[1];
+    meas[3 * c + 2] = slot[2];
+    *counter = c + 1;
 }
 __global__ void k_diag_philox(uint4 ctr, uint2 key, int n, uint4* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -679,6 +813,9 @@ int qcb_flow_create(qcb_field src, double eps, int prec, int store, qcb_flow* ou
 int qcb_flow_destroy(qcb_flow fl) {
     if (!fl) return QCB_OK;
     if (fl->fld && fl->fld->stream) cudaStreamSynchronize(fl->fld->stream);
+    drop_flow_graphs(fl);
+    if (fl->d_meas) cudaFree(fl->d_meas);
+    if (fl->d_count) cudaFree(fl->d_count);
     if (fl->z) cudaFree(fl->z);
     qcb_field_destroy(fl->fld);
     delete fl;
@@ -692,6 +829,10 @@ int qcb_flow_copy(qcb_flow fl, qcb_field src) {
 
 int qcb_flow_rk3(qcb_flow fl, int n) {
     if (!fl || n < 0) return fail(QCB_EINVAL, "invalid argument");
+    if (graphs_ok(fl->fld) && n >= 2) {
+        RET(ensure_alt(fl->fld));
+        for (; n >= 2; n -= 2) RET(flow_graph_run(fl, 1, 0));
+    }
     for (int i = 0; i < n; i++) RET(flow_step(fl));
     return QCB_OK;
 }
@@ -700,21 +841,29 @@ int qcb_flow_measure(qcb_flow fl, qcb_field src, int n_steps, int n_rk, double* 
     if (!fl || !src || !tQE || n_steps < 1 || n_rk < 0) return fail(QCB_EINVAL, "invalid argument");
     qcb_field_s* f = fl->fld;
     RET(qcb_field_copy(f, src));
-    double* d_meas = nullptr;
-    CK(cudaMallocAsync((void**)&d_meas, (size_t)n_steps * 3 * sizeof(double), f->stream));
-    int r = QCB_OK;
-    for (int s = 0; s < n_steps && r == QCB_OK; s++) {
-        r = enq_clover(f, d_meas + 3 * s);  // q, e and the plaquette sum
-        if (r == QCB_OK && s != n_steps - 1) r = qcb_flow_rk3(fl, n_rk);
+    if ((size_t)n_steps > fl->meas_cap) {
+        CK(cudaStreamSynchronize(f->stream));
+        if (fl->d_meas) cudaFree(fl->d_meas);
+        fl->d_meas = nullptr;
+        fl->meas_cap = 0;
+        CK(cudaMalloc(&fl->d_meas, (size_t)n_steps * 3 * sizeof(double)));
+        fl->meas_cap = (size_t)n_steps;
+    }
+    if (!fl->d_count) CK(cudaMalloc(&fl->d_count, sizeof(int)));
+    RET(ensure_alt(f));
+    RET(ensure_partials(f, (size_t)(((f->g.Vh + 127) / 128 < 65535 ? (f->g.Vh + 127) / 128 : 65535) * 18)));
+    CK(cudaMemsetAsync(fl->d_count, 0, sizeof(int), f->stream));
+    const bool graphs = graphs_ok(f) && n_rk > 0;
+    for (int s = 0; s < n_steps; s++) {
+        // measure (q, e and the plaquette sum), then n_rk RK3 steps unless this is the last time
+        if (graphs && s != n_steps - 1)
+            RET(flow_graph_run(fl, 2, n_rk));
+        else
+            RET(meas_block(fl, s != n_steps - 1 ? n_rk : 0));
     }
     std::vector<double> h((size_t)n_steps * 3);
-    if (r == QCB_OK) {
-        cudaError_t e = cudaMemcpyAsync(h.data(), d_meas, h.size() * sizeof(double), cudaMemcpyDeviceToHost, f->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
-        if (e != cudaSuccess) r = fail(QCB_ECUDA, "flow measure readback: %s", cudaGetErrorString(e));
-    }
-    cudaFreeAsync(d_meas, f->stream);
-    RET(r);
+    CK(cudaMemcpyAsync(h.data(), fl->d_meas, h.size() * sizeof(double), cudaMemcpyDeviceToHost, f->stream));
+    CK(cudaStreamSynchronize(f->stream));
     double t = 0.0;
     for (int s = 0; s < n_steps; s++) {
         tQE[3 * s] = t;
@@ -794,6 +943,39 @@ int qcb_diag_exp_su3(const double* Z, int n, double coeff, int prec, double* out
     cudaFree(dz);
     cudaFree(dout);
     if (e != cudaSuccess) return fail(QCB_ECUDA, "diag exp: %s", cudaGetErrorString(e));
+    return QCB_OK;
+}
+
+int qcb_diag_fma_rate(int prec, double* flop_per_s) {
+    if (!flop_per_s || (prec != QCB_PREC_F64 && prec != QCB_PREC_F32)) return fail(QCB_EINVAL, "invalid argument");
+    void* out = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaMalloc(&out, sizeof(double)));
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    const int blocks = sm_count() * 8, threads = 256;
+    const int iters = prec == QCB_PREC_F64 ? 1024 : 4096;
+    float best = 0.f;
+    for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {
+        e = cudaEventRecord(e0, 0);
+        if (prec == QCB_PREC_F64)
+            k_fma_rate<double><<<blocks, threads>>>(0.999999, 1e-7, iters, (double*)out);
+        else
+            k_fma_rate<float><<<blocks, threads>>>(0.999999f, 1e-7f, iters, (float*)out);
+        g_launches.fetch_add(1);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventRecord(e1, 0);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e == cudaSuccess && rep > 0 && (best == 0.f || ms < best)) best = ms;  // rep 0 warms up
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(out);
+    if (e != cudaSuccess) return fail(QCB_ECUDA, "fma rate: %s", cudaGetErrorString(e));
+    const double fmas = (double)blocks * threads * iters * 4.0 * 8.0;
+    *flop_per_s = 2.0 * fmas / (best * 1e-3);
     return QCB_OK;
 }
 

@@ -78,11 +78,30 @@ struct qcb_field_s {
     double t_ms[QCB_K_NCLASS] = {0};
 };
 
+// A captured sequence of a flow's launches, replayed with cudaGraphLaunch.  The launches bake in
+// device pointers, so a graph is reused only for the same buffers: the link buffer it starts from,
+// the reduction partials and the measurement buffer.
+struct FlowGraph {
+    cudaGraphExec_t exec = nullptr;
+    int kind = 0;  // 1: two RK3 steps; 2: one measurement + n_rk RK3 steps
+    int n_rk = 0;
+    int kernels = 0;  // kernels one replay launches
+    const void* links = nullptr;
+    const void* partials = nullptr;
+    const void* meas = nullptr;
+    uint64_t last_use = 0;
+};
+
 struct qcb_flow_s {
     qcb_field_s* fld = nullptr;  // flowed field (owned); fld->links holds W
     void* wtmp = nullptr;         // ping-pong partner of fld->links
     void* z = nullptr;            // su(3) accumulator, 8 reals per link
     double eps = 0.02;
+    double* d_meas = nullptr;     // measurement rows (t-independent: q, e, plaquette sums) of qcb_flow_measure
+    size_t meas_cap = 0;          // rows
+    int* d_count = nullptr;       // device row counter of the measurement graphs
+    FlowGraph graphs[4];
+    uint64_t graph_clock = 0;
 };
 
 namespace qcb {

@@ -883,8 +883,20 @@ __device__ __forceinline__ CloverF<R> clover_F(const LinkField<R, NE>& U, const 
 
 // Re Tr(Fa Fb) and |F|^2 of anti-Hermitian matrices from their nine reals:
 //   Re Tr(Fa Fb) = -2 sum_k Re(oa_k conj(ob_k)) - sum_i da_i db_i,  |F|^2 = 2 sum_k |o_k|^2 + sum_i d_i^2.
+#ifndef QCB_CLOVER32_SITE
+#define QCB_CLOVER32_SITE 0
+#endif
 template <typename R>
 __device__ __forceinline__ double clover_re_tr(const CloverF<R>& a, const CloverF<R>& b) {
+    if constexpr (sizeof(R) == 4 && QCB_CLOVER32_SITE) {
+        float s = 0.f, t = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            s = fmaf(a.o[k].re, b.o[k].re, fmaf(a.o[k].im, b.o[k].im, s));
+            t = fmaf(a.d[k], b.d[k], t);
+        }
+        return (double)(-2.f * s - t);
+    }
     double s = 0.0, t = 0.0;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -895,6 +907,15 @@ __device__ __forceinline__ double clover_re_tr(const CloverF<R>& a, const Clover
 }
 template <typename R>
 __device__ __forceinline__ double clover_sq_norm(const CloverF<R>& a) {
+    if constexpr (sizeof(R) == 4 && QCB_CLOVER32_SITE) {
+        float s = 0.f, t = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            s = fmaf(a.o[k].re, a.o[k].re, fmaf(a.o[k].im, a.o[k].im, s));
+            t = fmaf(a.d[k], a.d[k], t);
+        }
+        return (double)(2.f * s + t);
+    }
     double s = 0.0, t = 0.0;
 #pragma unroll
     for (int k = 0; k < 3; k++) {

@@ -23,6 +23,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -97,6 +98,20 @@ struct qcb_server_s {
     size_t partials_cap = 0;
     double2* staging = nullptr;
     size_t staging_cap = 0;
+    // CUDA graphs of the small requests' shared launches: one tick's measurement (clover pass,
+    // per-request finalize, tick counter) and its n_rk RK3 steps, captured for the resident set of
+    // `version` and the buffer parity the tick starts from, replayed while the set is unchanged
+    std::atomic<bool> graphs{true};
+    uint64_t version = 0;       // bumped by every rebuild of the work list
+    uint64_t version_ticks = 0;  // ticks measured with the current version
+    struct TickGraph {
+        cudaGraphExec_t exec = nullptr;
+        uint64_t version = 0;
+        int kernels = 0;
+    } gmeas[2], gflow[2];
+    int* d_tick = nullptr;  // the tick the device's finalize kernels write (advanced on the device)
+    int tick_dev = 0;       // the value d_tick holds once the enqueued work has run
+    int tick_copy = 0;      // host source of a d_tick reset
     // counters
     int tick = 0;       // measurements taken by the scheduler (slot index base)
     uint64_t nflow = 0; // RK3 steps executed (buffer parity)
@@ -112,8 +127,10 @@ namespace {
 // Per-request deterministic sums of clover partials, stored in the request's slot of this tick:
 // meas[(tick - tick0) * 3 + k] = (Q, sum e) (k = 0, 1; slot k = 2 is the plaquette sum, which
 // only the single-lattice path measures).
-__global__ void k_meas_finalize(const LatDesc* __restrict__ lats, const double* __restrict__ partials, int tick) {
+__global__ void k_meas_finalize(const LatDesc* __restrict__ lats, const double* __restrict__ partials,
+                                const int* __restrict__ d_tick) {
     __shared__ double sm[256];
+    const int tick = *d_tick;
     const LatDesc* d = lats + blockIdx.x;
     const int t0 = 6 * d->nb_begin, nt = 6 * d->nb;
     for (int k = 0; k < 2; k++) {
@@ -129,6 +146,9 @@ __global__ void k_meas_finalize(const LatDesc* __restrict__ lats, const double* 
         __syncthreads();
     }
 }
+
+// Advances the device tick counter after a tick's finalize kernels have read it.
+__global__ void k_tick_bump(int* d_tick) { *d_tick += 1; }
 
 int set_error(qcb_server_s* s, int code, const std::string& msg) {
     std::lock_guard<std::mutex> lk(s->mu);
@@ -160,6 +180,8 @@ bool grow(qcb_server_s* s, T** p, size_t* cap, size_t n) {
 
 // Rebuilds the descriptors and tile map of the active set.
 bool rebuild(qcb_server_s* s) {
+    s->version++;
+    s->version_ticks = 0;
     s->desc.clear();
     s->small.clear();
     s->big.clear();
@@ -273,6 +295,69 @@ bool flow_big(qcb_server_s* s, Request* r, int stage, int flip_xor, int rep) {
                    "flow launch");
 }
 
+// The small requests' measurement of one tick: batched clover pass, per-request finalize into each
+// request's slot of the device tick, tick counter advanced.  Returns the kernels launched (or -1).
+int small_measure(qcb_server_s* s, const WorkList& w, int fx) {
+    if (!cuda_ok(s, fmt_ops(s->fmt).clover_tiles(w, fx, s->partials, s->stream_small), "clover launch")) return -1;
+    k_meas_finalize<<<(unsigned)s->small.size(), 256, 0, s->stream_small>>>(s->d_desc, s->partials, s->d_tick);
+    k_tick_bump<<<1, 1, 0, s->stream_small>>>(s->d_tick);
+    return cuda_ok(s, cudaGetLastError(), "measure finalize") ? 3 : -1;
+}
+// The small requests' n_rk RK3 steps, from buffer parity f0.
+int small_flow(qcb_server_s* s, const WorkList& w, int f0, int rep) {
+    for (int k = 0; k < s->n_rk; k++)
+        for (int stage = 1; stage <= 3; stage++)
+            if (!cuda_ok(s, fmt_ops(s->fmt).flow(w, stage, (f0 + k) & 1, rep, s->stream_small), "flow launch"))
+                return -1;
+    return 3 * s->n_rk;
+}
+
+// Runs body (small_measure or small_flow) for parity fx: plainly on the first tick of a resident
+// set (or with graphs off), else by replaying the graph captured from the same set and parity.
+template <class Body>
+bool small_run(qcb_server_s* s, qcb_server_s::TickGraph cache[2], int fx, Body body) {
+    if (!s->graphs.load() || s->version_ticks < 1) {
+        const int k = body();
+        if (k < 0) return false;
+        note_launches(k);
+        return true;
+    }
+    qcb_server_s::TickGraph& g = cache[fx];
+    if (!g.exec || g.version != s->version) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = qcb_server_s::TickGraph{};
+        cudaGraph_t graph = nullptr;
+        if (!cuda_ok(s, cudaStreamBeginCapture(s->stream_small, cudaStreamCaptureModeThreadLocal), "tick capture"))
+            return false;
+        const int k = body();
+        const cudaError_t e = cudaStreamEndCapture(s->stream_small, &graph);
+        if (k < 0) {
+            if (graph) cudaGraphDestroy(graph);
+            return false;
+        }
+        if (!cuda_ok(s, e, "tick capture end")) return false;
+        const cudaError_t ei = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (!cuda_ok(s, ei, "tick graph instantiate")) {
+            g.exec = nullptr;
+            return false;
+        }
+        g.version = s->version;
+        g.kernels = k;
+    }
+    if (!cuda_ok(s, cudaGraphLaunch(g.exec, s->stream_small), "tick graph launch")) return false;
+    note_launches(g.kernels);
+    return true;
+}
+
+void drop_tick_graphs(qcb_server_s* s) {
+    for (auto* c : {s->gmeas, s->gflow})
+        for (int i = 0; i < 2; i++) {
+            if (c[i].exec) cudaGraphExecDestroy(c[i].exec);
+            c[i] = qcb_server_s::TickGraph{};
+        }
+}
+
 void scheduler(qcb_server_s* s) {
     cudaSetDevice(s->device);
     const int rep = needs_reproject(s->prec, s->store);
@@ -308,12 +393,16 @@ void scheduler(qcb_server_s* s) {
         w.nlat = (int)s->small.size();
         const int fx = (int)(s->nflow & 1);
         if (!s->small.empty()) {
-            if (!cuda_ok(s, fmt_ops(s->fmt).clover_tiles(w, fx, s->partials, s->stream_small), "clover launch"))
-                break;
-            k_meas_finalize<<<(unsigned)s->small.size(), 256, 0, s->stream_small>>>(s->d_desc, s->partials, s->tick);
-            if (!cuda_ok(s, cudaGetLastError(), "measure finalize")) break;
-            note_launches(2);
+            if (s->tick_dev != s->tick) {  // ticks without small requests left the device counter behind
+                s->tick_copy = s->tick;
+                if (!cuda_ok(s, cudaMemcpyAsync(s->d_tick, &s->tick_copy, sizeof(int), cudaMemcpyHostToDevice,
+                                                s->stream_small), "tick counter"))
+                    break;
+            }
+            if (!small_run(s, s->gmeas, fx, [&] { return small_measure(s, w, fx); })) break;
+            s->tick_dev = s->tick + 1;
         }
+        s->version_ticks++;
         for (Request* r : s->big) ok = ok && measure_big(s, r, fx);
         if (!ok) break;
         // requests that took their last measurement leave the mix
@@ -330,16 +419,16 @@ void scheduler(qcb_server_s* s) {
             w.nb_total = s->nb_total;
             w.nlat = (int)s->small.size();
         }
-        for (int k = 0; k < s->n_rk && !s->active.empty() && ok; k++) {
-            const int f = (int)(s->nflow & 1);
-            for (int stage = 1; stage <= 3 && ok; stage++) {
-                if (!s->small.empty()) {
-                    ok = cuda_ok(s, fmt_ops(s->fmt).flow(w, stage, f, rep, s->stream_small), "flow launch");
-                    note_launches(1);
-                }
-                for (Request* r : s->big) ok = ok && flow_big(s, r, stage, f, rep);
+        if (!s->active.empty()) {
+            const int f0 = (int)(s->nflow & 1);
+            if (!s->small.empty())
+                ok = small_run(s, s->gflow, f0, [&] { return small_flow(s, w, f0, rep); });
+            for (int k = 0; k < s->n_rk && ok; k++) {
+                const int f = (f0 + k) & 1;
+                for (int stage = 1; stage <= 3 && ok; stage++)
+                    for (Request* r : s->big) ok = ok && flow_big(s, r, stage, f, rep);
             }
-            s->nflow++;
+            s->nflow += (uint64_t)s->n_rk;
         }
         if (!ok) break;
         {
@@ -357,6 +446,7 @@ void scheduler(qcb_server_s* s) {
     }
     cudaStreamSynchronize(s->stream);
     cudaStreamSynchronize(s->stream_small);
+    drop_tick_graphs(s);
 }
 
 }  // namespace
@@ -380,6 +470,8 @@ int qcb_serve_create(size_t hbm_budget_bytes, int prec, int store, int n_rk, int
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream_small, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_layout, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_tick, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(s->d_tick, 0, sizeof(int));
     if (e == cudaSuccess) {
         cudaMemPoolProps props;
         memset(&props, 0, sizeof(props));
@@ -421,6 +513,7 @@ int qcb_serve_destroy(qcb_server s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->stream_small) cudaStreamSynchronize(s->stream_small);
     if (s->ev_layout) cudaEventDestroy(s->ev_layout);
+    if (s->d_tick) cudaFree(s->d_tick);
     if (s->d_desc) cudaFree(s->d_desc);
     if (s->d_tile_lat) cudaFree(s->d_tile_lat);
     if (s->partials) cudaFree(s->partials);
@@ -431,6 +524,15 @@ int qcb_serve_destroy(qcb_server s) {
     if (s->stream_small) cudaStreamDestroy(s->stream_small);
     delete s;
     return QCB_OK;
+}
+
+int qcb_serve_set_option(qcb_server s, int option, int value) {
+    if (!s) return fail(QCB_EINVAL, "null server");
+    if (option == QCB_SERVE_GRAPHS) {
+        s->graphs.store(value != 0);
+        return QCB_OK;
+    }
+    return fail(QCB_EINVAL, "unknown server option %d", option);
 }
 
 double qcb_serve_now(qcb_server s) { return s ? s->now() : 0.0; }

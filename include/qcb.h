@@ -198,6 +198,11 @@ int qcb_debug_probe_link(qcb_field f, int mu, int parity, int64_t h);
 int qcb_diag_staple(qcb_field f, int mu, double* out);
 /* exp_su3_luscher (src/su3/utils.cpp:145-193) of n matrices (n*9 complex) on the device. */
 int qcb_diag_exp_su3(const double* Z, int n, double coeff, int prec, double* out);
+/* Measured fused multiply-add throughput of the current device in FLOP/s (2 per FMA), FP64 or FP32
+ * (prec = QCB_PREC_F64 / QCB_PREC_F32): independent FMA chains on every SM, best of three timed
+ * launches after a warm-up, on the legacy default stream.  The denominator of the flow kernels'
+ * pipe fractions.  No counterpart in the reference. */
+int qcb_diag_fma_rate(int prec, double* flop_per_s);
 /* n Philox4x32-10 blocks on the device: ctr word 0 = ctr[0] + i. */
 int qcb_diag_philox(const uint32_t ctr[4], const uint32_t key[2], int n, uint32_t* out);
 
@@ -241,6 +246,12 @@ int qcb_batch_tune(qcb_batch b, int n_hits, int n_trial, int allow_store_change,
  * max_active <= 0: no limit besides the budget. */
 int qcb_serve_create(size_t hbm_budget_bytes, int prec, int store, int n_rk, int max_active, qcb_server* out);
 int qcb_serve_destroy(qcb_server s);
+/* Server options.  QCB_SERVE_GRAPHS (default 1): while the resident set of small requests is
+ * unchanged from one tick to the next, their shared launches of a tick (the batched clover pass with
+ * its per-request finalize, and the n_rk RK3 steps) are replayed from CUDA graphs captured for that
+ * set; 0 launches them one by one.  Results are the same either way. */
+#define QCB_SERVE_GRAPHS 1
+int qcb_serve_set_option(qcb_server s, int option, int value);
 /* Seconds on the server's clock (the clock of the times returned by qcb_serve_poll). */
 double qcb_serve_now(qcb_server s);
 /* Queues one request (thread-safe): host AoS FP64 links of an L[0..3] lattice, flow step eps,

@@ -310,3 +310,30 @@ def test_invalid_arguments(gpu):
         f.hb_subsweep(6.0, 1, 1, 0, 2, 0)
     with pytest.raises(gpu.QcbError):
         f.hb_subsweep(-1.0, 1, 1, 0, 0, 0)
+
+
+@pytest.mark.parametrize("prec,store", [(64, 0), (64, 1), (32, 0), (32, 1)])
+def test_flow_graphs_match_plain_launches(gpu, orc, prec, store):
+    """qcb_flow_rk3 and qcb_flow_measure replay captured CUDA graphs (pairs of RK3 steps; measurement
+    blocks) unless per-launch timing is on, in which case every stage is a plain launch.  Both ways
+    run the same kernels with the same arguments: the flowed links and every (t, Q, E, P) agree bit for
+    bit, for odd and even step counts and for n_rk = 1, 2, 3 (graph replays from either buffer)."""
+    L = (8, 8, 8, 8)
+    U = orc.hot_start(L, 3)
+    orc.hb_sweep(U, L, 6.0, 1, 3, 0)
+    f = gpu.GaugeField(L, 64, 0)
+    f.upload(U)
+    a = gpu.GradientFlow(f, 0.02, prec=prec, store=store)
+    b = gpu.GradientFlow(f, 0.02, prec=prec, store=store)
+    b.field.timing(True)
+    n0 = gpu.launch_count()
+    for n in (5, 4, 1, 2):
+        a.rk3_step(n)
+        b.rk3_step(n)
+        assert np.array_equal(a.field.download(), b.field.download()), n
+    assert gpu.launch_count() - n0 >= 2 * 3 * 12  # every stage counted, replayed or not
+    for n_rk in (1, 2, 3, 1):
+        ta, pa = a.measure(f, 6, n_rk, plaquette=True)
+        tb, pb = b.measure(f, 6, n_rk, plaquette=True)
+        assert np.array_equal(ta, tb) and np.array_equal(pa, pb), n_rk
+        assert np.array_equal(a.field.download(), b.field.download()), n_rk

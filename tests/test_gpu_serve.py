@@ -121,3 +121,23 @@ def test_big_request_single_lattice_path(gpu):
     mix = run(s, [(1, f.L, U, 4), (2, g.L, Ug, 6), (3, g.L, Ug, 3)])
     assert np.array_equal(mix[1][1], alone)
     assert s.stats()["peak_resident"] >= 2
+
+
+@pytest.mark.parametrize("n_rk", [1, 2])
+def test_tick_graphs_match_plain_launches(gpu, n_rk):
+    """While the resident set of small requests is unchanged, their shared launches of a tick are
+    replayed from CUDA graphs; every result equals the one-by-one launches' bit for bit (requests
+    leaving at different ticks change the set, so both paths and the recaptures are exercised)."""
+    reqs = []
+    for i, (L, n) in enumerate([((8, 8, 8, 8), 9), ((12, 12, 12, 12), 5), ((8, 8, 8, 8), 14), ((4, 6, 2, 8), 7)]):
+        _, U = config(gpu, L, 40 + i)
+        reqs.append((i, L, U, n))
+    out = {}
+    for on in (True, False):
+        s = gpu.Server(1 << 30, prec=32, store=0, n_rk=n_rk)
+        s.set_graphs(on)
+        out[on] = run(s, reqs)
+        s.close()
+    assert set(out[True]) == set(out[False]) == {0, 1, 2, 3}
+    for rid in range(4):
+        assert np.array_equal(out[True][rid][1], out[False][rid][1]), rid
