@@ -140,6 +140,8 @@ int check_err_flag(qcb_field_s* f) {
     CK(cudaStreamSynchronize(f->stream));
     if (h) {
         CK(cudaMemsetAsync(f->d_err, 0, sizeof(int), f->stream));
+        if (h & DERR_BULK_WAIT)
+            return fail(QCB_ETIMEOUT, "heatbath: bulk copy of the block's links did not complete (links left unchanged)");
         if (h & DERR_KP_SCALE)
             return fail(QCB_ERANGE, "heatbath: zero or non-finite SU(2) projection of the staple (link left unchanged)");
         return fail(QCB_ERANGE, "heatbath: Kennedy-Pendleton attempt cap (2^20) reached (link left unchanged)");
@@ -167,8 +169,7 @@ int enq_plaquette(qcb_field_s* f, double* dst) {
 // pass sweeps the lattice once in t and a link's neighbours are still in L2 when the front reaches
 // them (a capped grid-stride loop jumps across the lattice and re-reads them from DRAM).
 int enq_clover(qcb_field_s* f, double* dst) {
-    const int64_t nb_all = ((int64_t)f->g.Vh + 127) / 128;
-    const unsigned nbx = (unsigned)(nb_all < 65535 ? nb_all : 65535);
+    const unsigned nbx = clover_blocks(f->g.Vh);
     RET(ensure_partials(f, (size_t)nbx * 6 * 3));
     RET(launch(f, QCB_K_CLOVER, [&] { return fmt_ops(f->fmt).clover(f->g, f->links, f->partials, nbx, f->stream); }));
     return finalize(f, (int)(nbx * 6), 3, 0u, dst);
@@ -851,7 +852,7 @@ int qcb_flow_measure(qcb_flow fl, qcb_field src, int n_steps, int n_rk, double* 
     }
     if (!fl->d_count) CK(cudaMalloc(&fl->d_count, sizeof(int)));
     RET(ensure_alt(f));
-    RET(ensure_partials(f, (size_t)(((f->g.Vh + 127) / 128 < 65535 ? (f->g.Vh + 127) / 128 : 65535) * 18)));
+    RET(ensure_partials(f, (size_t)clover_blocks(f->g.Vh) * 18));
     CK(cudaMemsetAsync(fl->d_count, 0, sizeof(int), f->stream));
     const bool graphs = graphs_ok(f) && n_rk > 0;
     for (int s = 0; s < n_steps; s++) {

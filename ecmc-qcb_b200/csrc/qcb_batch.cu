@@ -163,6 +163,8 @@ int read_err(qcb_batch_s* b) {
     CK(cudaStreamSynchronize(b->stream));
     if (h) {
         CK(cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream));
+        if (h & DERR_BULK_WAIT)
+            return fail(QCB_ETIMEOUT, "heatbath: bulk copy of the block's links did not complete (links left unchanged)");
         if (h & DERR_KP_SCALE)
             return fail(QCB_ERANGE, "batch heatbath: zero or non-finite SU(2) projection of a staple");
         return fail(QCB_ERANGE, "batch heatbath: Kennedy-Pendleton attempt cap (2^20) reached");

@@ -34,6 +34,14 @@ inline bool lattice_ok(const int* L, int64_t* V_out = nullptr) {
     return true;
 }
 
+// Site blocks (grid y) of the single-lattice clover pass: one block of 128 threads per 128 half-sites,
+// up to the grid's y limit (a grid-stride loop covers the rest).  Every clover pass of a lattice uses
+// this count, so its partial sums and their order are the same on every path.
+inline unsigned clover_blocks(int64_t Vh) {
+    const int64_t nb = (Vh + 127) / 128;
+    return (unsigned)(nb < 65535 ? nb : 65535);
+}
+
 int fail(int code, const char* fmt, ...);
 // Adds n to the process-wide kernel launch counter reported by qcb_launch_count().
 void note_launches(int n);

@@ -12,7 +12,41 @@ namespace qcb {
 constexpr double kPi = 3.14159265358979323846;
 
 // Device error flags (bit mask written by kernels, read by the host after a sync).
-enum : int { DERR_KP_CAP = 1, DERR_KP_SCALE = 2 };
+enum : int { DERR_KP_CAP = 1, DERR_KP_SCALE = 2, DERR_BULK_WAIT = 4 };
+
+// ------------------------------------------------------------------ bulk copies into shared memory
+// One-shot mbarrier-tracked bulk copies (the TMA engine's cp.async.bulk, global -> this CTA's shared
+// memory, no multicast).  Addresses 16-byte aligned, sizes multiples of 16 bytes.
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst), b = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
+                 "l"(src), "r"(bytes), "r"(b)
+                 : "memory");
+}
+// Waits for phase `phase` of the barrier, at most max_tries polls (each poll may suspend the thread
+// for a bounded, hardware-chosen time); false if the copies did not land in that time.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase, int max_tries) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    for (int i = 0; i < max_tries; i++) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(a), "r"(phase)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
 
 // byte reversal of a double (ILDG files are big-endian, src/io/ildg.cpp:25-32)
 __device__ __forceinline__ double bswap_f64(double x) {
@@ -218,6 +252,9 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
 #endif
 #ifndef QCB_HB_MINB
 #define QCB_HB_MINB(R) (sizeof(R) == 8 ? 4 : 6)
+#endif
+#ifndef QCB_HB_BULK_LINKS
+#define QCB_HB_BULK_LINKS 0
 #endif
 #ifndef QCB_FLOW_THREADS
 #define QCB_FLOW_THREADS 128
@@ -533,7 +570,7 @@ __device__ __forceinline__ void cm_subgroup_rt(const StapleSlot<R>& u, const Sta
 template <typename R, int NE, int MU, bool SLOT>
 __device__ __forceinline__ void hb_link(const Geom& g, const LinkField<R, NE>& U, int par, int h, double c_alpha,
                                         int n_hits, uint64_t seed, uint32_t sweep, int reproject, int* err,
-                                        typename V2<R>::T* slot, int slot_stride) {
+                                        typename V2<R>::T* slot, int slot_stride, uint64_t* link_bar = nullptr) {
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
     const int lex = lex_of(g, c);
@@ -543,7 +580,15 @@ __device__ __forceinline__ void hb_link(const Geom& g, const LinkField<R, NE>& U
         const StapleSlot<R> S{slot, slot_stride}, Us{slot + 9 * slot_stride, slot_stride};
         staple_rows_into<R, NE>(g, U, c, lex, par, MU, S);
         KPDraws d = kp_draws_at(rng, 0u);
-        Us.put(U.load(MU, par, h));
+        if (link_bar) {
+            // the block's own links were bulk-copied into the link slots while the staple was formed
+            if (!mbar_wait(link_bar, 0u, 1 << 20)) {
+                atomicOr(err, (int)DERR_BULK_WAIT);
+                return;  // link left unchanged; the host reports the error
+            }
+        } else {
+            Us.put(U.load(MU, par, h));
+        }
         const int n_sub = 3 * n_hits;
 #pragma unroll 1
         for (int it = 0; it < n_sub; it++) {
@@ -577,12 +622,34 @@ template <typename R, int NE, int MU>
 __global__ void __launch_bounds__(QCB_HB_THREADS, QCB_HB_MINB(R))
     k_hb_subsweep(Geom g, LinkField<R, NE> U, int par, double c_alpha, int n_hits, uint64_t seed, uint32_t sweep,
                   int reproject, int* err) {
-    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= g.Vh) return;
     static_assert(HbSlotFits<R, QCB_HB_THREADS>::value, "heatbath slot exceeds static shared memory");
     __shared__ typename V2<R>::T slot[18 * QCB_HB_THREADS];
+    uint64_t* link_bar = nullptr;
+#if QCB_HB_BULK_LINKS
+    // FP64 18-real: the block's own links U_mu(par, h) for its 128 half-sites are 4 whole 32-site
+    // tiles, element-major within a tile -- exactly the element-major layout of the link slots --
+    // so one thread bulk-copies them there (36 copies of 512 B; tiles past the field are skipped)
+    // and the copies land while the staple is formed.
+    __shared__ __align__(8) uint64_t bar;
+    if constexpr (sizeof(R) == 8 && NE == 9 && QCB_HB_THREADS == 128) {
+        if (threadIdx.x == 0) mbar_init(&bar, 1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int nT = (int)((g.Vh + 31) >> 5);
+            const int t0 = blockIdx.x * 4, t1 = min(t0 + 4, nT);
+            mbar_expect_tx(&bar, (unsigned)((t1 - t0) * 9 * 32 * sizeof(double2)));
+            for (int t = t0; t < t1; t++)
+                for (int e = 0; e < 9; e++)
+                    bulk_copy_g2s(slot + (9 + e) * 128 + (t - t0) * 32, U.p + U.tile0(MU, par, t * 32) + e * 32,
+                                  32 * sizeof(double2), &bar);
+        }
+        link_bar = &bar;
+    }
+#endif
+    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= g.Vh) return;
     hb_link<R, NE, MU, true>(g, U, par, (int)h, c_alpha, n_hits, seed, sweep, reproject, err, slot + threadIdx.x,
-                             QCB_HB_THREADS);
+                             QCB_HB_THREADS, link_bar);
 }
 
 // One link's heatbath update (the C ABI's single-link entry, qcb_hb_link; reference
@@ -883,8 +950,11 @@ __device__ __forceinline__ CloverF<R> clover_F(const LinkField<R, NE>& U, const 
 
 // Re Tr(Fa Fb) and |F|^2 of anti-Hermitian matrices from their nine reals:
 //   Re Tr(Fa Fb) = -2 sum_k Re(oa_k conj(ob_k)) - sum_i da_i db_i,  |F|^2 = 2 sum_k |o_k|^2 + sum_i d_i^2.
+// FP32 clover pass: the per-site traces Re Tr(Fa Fb) and |F|^2 in FP32 (the global sums of q, e
+// and the plaquette stay FP64): 0.341 against 0.348 ms at 32^4, with the site values' FP32 rounding
+// (~1e-7 relative) far inside the |dQ| < 1e-4 and dE/E < 1e-6 bounds of the FP32 forms.
 #ifndef QCB_CLOVER32_SITE
-#define QCB_CLOVER32_SITE 0
+#define QCB_CLOVER32_SITE 1
 #endif
 template <typename R>
 __device__ __forceinline__ double clover_re_tr(const CloverF<R>& a, const CloverF<R>& b) {

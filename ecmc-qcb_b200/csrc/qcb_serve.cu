@@ -270,8 +270,7 @@ void* current_links(const Request* r, int flip_xor) {
 // Clover Q/E (and plaquette) of a big request with the single-lattice kernel, summed into its
 // measurement slot of this tick.
 bool measure_big(qcb_server_s* s, Request* r, int flip_xor) {
-    const int64_t need = (r->g.Vh + 127) / 128;
-    const unsigned nbx = (unsigned)std::min<int64_t>(need, 148 * 8);
+    const unsigned nbx = clover_blocks(r->g.Vh);
     if (!grow(s, &s->big_partials, &s->big_partials_cap, (size_t)nbx * 6 * 3)) return false;
     if (!cuda_ok(s, fmt_ops(s->fmt).clover(r->g, current_links(r, flip_xor), s->big_partials, nbx, s->stream),
                  "clover launch"))
