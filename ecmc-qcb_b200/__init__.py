@@ -77,6 +77,9 @@ def exported_symbols():
         "qcb_flow_rk3": (i, [_vp, i]),
         "qcb_flow_measure": (i, [_vp, _vp, i, i, _vp, _vp]),
         "qcb_flow_field": (_vp, [_vp]),
+        "qcb_flow_pass": (i, [_vp, i]),
+        "qcb_clover_site": (i, [_vp, C.c_int64, i, i, _vp]),
+        "qcb_local_qe": (i, [_vp, C.c_int64, pd, pd]),
         "qcb_ildg_write": (i, [_vp, C.c_char_p]),
         "qcb_ildg_read": (i, [_vp, C.c_char_p]),
         "qcb_ildg_probe": (i, [C.c_char_p, _i4, pi]),
@@ -275,6 +278,18 @@ class GaugeField:
     def clover_qe(self):
         q, e = C.c_double(), C.c_double()
         _check(lib().qcb_clover_qe(self.h, C.byref(q), C.byref(e)))
+        return q.value, e.value
+
+    def clover_site(self, site: int, mu: int, nu: int) -> np.ndarray:
+        """clover_site: F_mu_nu (3x3) at one lexicographic site."""
+        F = np.empty((3, 3), dtype=np.complex128)
+        _check(lib().qcb_clover_site(self.h, int(site), int(mu), int(nu), F.ctypes.data))
+        return F
+
+    def local_qe(self, site: int):
+        """local_q_e_clover at one lexicographic site: (q, e)."""
+        q, e = C.c_double(), C.c_double()
+        _check(lib().qcb_local_qe(self.h, int(site), C.byref(q), C.byref(e)))
         return q.value, e.value
 
     def staple(self, mu: int) -> np.ndarray:
@@ -489,6 +504,12 @@ class GradientFlow:
 
     def rk3_step(self, n: int = 1) -> None:
         _check(lib().qcb_flow_rk3(self.h, int(n)))
+
+    # the reference's separate member passes (compute_force, compute_w1/2/3, replace_force_0)
+    FORCE0, FORCE1, W1, W2, REPLACE_F0, W3 = range(6)
+
+    def run_pass(self, p: int) -> None:
+        _check(lib().qcb_flow_pass(self.h, int(p)))
 
     def measure(self, field: GaugeField, n_steps: int, n_rk: int = 1, plaquette: bool = False):
         """topo_charge_flowed: returns an (n_steps, 3) array of (t, Q, E), and plaquettes if asked."""

@@ -781,6 +781,44 @@ int qcb_clover_qe(qcb_field f, double* Q, double* E) {
     return QCB_OK;
 }
 
+// Lattice site (lexicographic index) -> (parity, half-site index); false outside the lattice.
+static bool site_of(const qcb_field_s* f, int64_t site, int* par, int* h) {
+    if (site < 0 || site >= f->g.V) return false;
+    int64_t r = site;
+    int p = 0;
+    for (int d = 0; d < 4; d++) {
+        p += (int)(r % f->L[d]);
+        r /= f->L[d];
+    }
+    *par = p & 1;
+    *h = (int)(site >> 1);
+    return true;
+}
+
+int qcb_clover_site(qcb_field f, int64_t site, int mu, int nu, double* F_out) {
+    int par = 0, h = 0;
+    if (!f || !F_out || !site_of(f, site, &par, &h) || mu < 0 || mu > 3 || nu < 0 || nu > 3 || mu == nu)
+        return fail(QCB_EINVAL, "clover site: site in [0, V), mu != nu in 0..3, non-null output");
+    RET(launch(f, QCB_K_CLOVER, [&] {
+        return fmt_ops(f->fmt).clover_site(f->g, f->links, par, h, mu, nu, f->d_res, f->stream);
+    }));
+    RET(read_results(f, 18));
+    memcpy(F_out, f->h_res, 18 * sizeof(double));
+    return QCB_OK;
+}
+
+int qcb_local_qe(qcb_field f, int64_t site, double* q, double* e) {
+    int par = 0, h = 0;
+    if (!f || !site_of(f, site, &par, &h)) return fail(QCB_EINVAL, "local q, e: site in [0, V)");
+    RET(launch(f, QCB_K_CLOVER, [&] {
+        return fmt_ops(f->fmt).clover_site(f->g, f->links, par, h, -1, -1, f->d_res, f->stream);
+    }));
+    RET(read_results(f, 2));
+    if (q) *q = f->h_res[0];
+    if (e) *e = f->h_res[1];
+    return QCB_OK;
+}
+
 // ------------------------------------------------------------------ flow
 int qcb_flow_create(qcb_field src, double eps, int prec, int store, qcb_flow* out) {
     if (!src || !out) return fail(QCB_EINVAL, "null argument");
@@ -815,6 +853,7 @@ int qcb_flow_destroy(qcb_flow fl) {
     if (!fl) return QCB_OK;
     if (fl->fld && fl->fld->stream) cudaStreamSynchronize(fl->fld->stream);
     drop_flow_graphs(fl);
+    if (fl->f1) cudaFree(fl->f1);
     if (fl->d_meas) cudaFree(fl->d_meas);
     if (fl->d_count) cudaFree(fl->d_count);
     if (fl->z) cudaFree(fl->z);
@@ -878,6 +917,39 @@ int qcb_flow_measure(qcb_flow fl, qcb_field src, int n_steps, int n_rk, double* 
 }
 
 qcb_field qcb_flow_field(qcb_flow fl) { return fl ? fl->fld : nullptr; }
+
+int qcb_flow_pass(qcb_flow fl, int pass) {
+    if (!fl || pass < QCB_FLOW_FORCE0 || pass > QCB_FLOW_W3) return fail(QCB_EINVAL, "flow pass: invalid argument");
+    qcb_field_s* f = fl->fld;
+    if ((pass == QCB_FLOW_FORCE1 || pass == QCB_FLOW_W2 || pass == QCB_FLOW_REPLACE_F0 || pass == QCB_FLOW_W3) &&
+        !fl->f1)
+        CK(cudaMalloc(&fl->f1, alg_bytes(f->fmt, f->g.Vh)));
+    const FmtOps& o = fmt_ops(f->fmt);
+    const int rep = needs_reproject(f->prec, f->store);
+    const double e = fl->eps;
+    switch (pass) {
+        case QCB_FLOW_FORCE0:
+        case QCB_FLOW_FORCE1:
+            return launch(f, QCB_K_FLOW, [&] {
+                return o.flow_force(f->g, f->links, pass == QCB_FLOW_FORCE0 ? fl->z : fl->f1, f->stream);
+            });
+        case QCB_FLOW_W1:
+            return launch(f, QCB_K_FLOW, [&] {
+                return o.flow_update(f->g, f->links, fl->z, nullptr, 0.25 * e, 0.0, 0, rep, f->stream);
+            });
+        case QCB_FLOW_W2:
+            return launch(f, QCB_K_FLOW, [&] {
+                return o.flow_update(f->g, f->links, fl->z, fl->f1, (8.0 / 9.0) * e, (17.0 / 36.0) * e, 1, rep,
+                                     f->stream);
+            });
+        case QCB_FLOW_REPLACE_F0:
+            return launch(f, QCB_K_FLOW, [&] { return o.flow_replace(f->g, fl->z, fl->f1, f->stream); });
+        default:
+            return launch(f, QCB_K_FLOW, [&] {
+                return o.flow_update(f->g, f->links, fl->z, fl->f1, 0.75 * e, e, 1, rep, f->stream);
+            });
+    }
+}
 
 // ------------------------------------------------------------------ instrumentation
 int qcb_timing_enable(qcb_field f, int on) {

@@ -121,6 +121,35 @@ struct FmtImpl {
         return cudaGetLastError();
     }
 
+    static AlgField<R> alg(const void* p, int64_t Vh) {
+        AlgField<R> z;
+        z.p = (typename AlgField<R>::C2*)p;
+        z.Vh = Vh;
+        return z;
+    }
+    static cudaError_t flow_force(const Geom& g, const void* w, void* f, cudaStream_t s) {
+        const unsigned nb = 8u * (unsigned)((g.Vh + QCB_FLOW1_THREADS - 1) / QCB_FLOW1_THREADS);
+        k_flow_force<R, NE><<<nb, QCB_FLOW1_THREADS, 0, s>>>(g, view(w, g.Vh), alg(f, g.Vh));
+        return cudaGetLastError();
+    }
+    static cudaError_t flow_update(const Geom& g, void* w, const void* f0, const void* f1, double a, double b,
+                                   int use_f1, int rep, cudaStream_t s) {
+        const dim3 grid((unsigned)((g.Vh + 255) / 256), 8);
+        k_flow_update<R, NE><<<grid, 256, 0, s>>>(g, view(w, g.Vh), alg(f0, g.Vh), alg(f1 ? f1 : f0, g.Vh), a, b,
+                                                  use_f1, rep);
+        return cudaGetLastError();
+    }
+    static cudaError_t flow_replace(const Geom& g, void* f0, const void* f1, cudaStream_t s) {
+        const dim3 grid((unsigned)((g.Vh + 255) / 256), 8);
+        k_flow_replace<R><<<grid, 256, 0, s>>>(g.Vh, alg(f0, g.Vh), alg(f1, g.Vh));
+        return cudaGetLastError();
+    }
+    static cudaError_t clover_site(const Geom& g, const void* links, int par, int h, int mu, int nu, double* out,
+                                   cudaStream_t s) {
+        k_clover_site<R, NE><<<1, 1, 0, s>>>(g, view(links, g.Vh), par, h, mu, nu, out);
+        return cudaGetLastError();
+    }
+
     // Reduction work lists are not persistent: one block per tile, one partial per tile.
     static cudaError_t plaq_tiles(const WorkList& w, int flip_xor, double* partials, cudaStream_t s) {
         const int ntiles = 2 * w.nb_total;
@@ -189,6 +218,10 @@ struct FmtImpl {
         o.hb_one = &hb_one;
         o.probe_link = &probe_link;
         o.flow1 = &flow1;
+        o.flow_force = &flow_force;
+        o.flow_update = &flow_update;
+        o.flow_replace = &flow_replace;
+        o.clover_site = &clover_site;
         o.plaquette = &plaquette;
         o.clover = &clover;
         o.unitarity = &unitarity;

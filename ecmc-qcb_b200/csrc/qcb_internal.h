@@ -103,7 +103,8 @@ struct FlowGraph {
 struct qcb_flow_s {
     qcb_field_s* fld = nullptr;  // flowed field (owned); fld->links holds W
     void* wtmp = nullptr;         // ping-pong partner of fld->links
-    void* z = nullptr;            // su(3) accumulator, 8 reals per link
+    void* z = nullptr;            // su(3) accumulator, 8 reals per link (force_0 of the separate passes)
+    void* f1 = nullptr;           // force_1 of the separate passes, allocated at their first use
     double eps = 0.02;
     double* d_meas = nullptr;     // measurement rows (t-independent: q, e, plaquette sums) of qcb_flow_measure
     size_t meas_cap = 0;          // rows

@@ -747,6 +747,62 @@ __global__ void __launch_bounds__(QCB_FLOW1_THREADS, QCB_FLOW1_MINB(R))
     flow_link<R, NE, STAGE>(g, Win, Wout, Z, eps, lt >> 1, lt & 1, (int)h, reproject);
 }
 
+// ------------------------------------------------------------------ the reference's separate flow passes
+// GradientFlow's member passes (src/flow/gradient_flow.cpp:17-121), for callers that drive them one
+// by one; rk3_step runs the fused stages above.  Forces are su(3) fields in the accumulator layout.
+// compute_force: F = proj_lie_su3(-U A) of every link, with the fused stage's staple and projection.
+// Grid: blockIdx.x = (site block) * 8 + (mu*2 + parity), as the fused stage.
+template <typename R, int NE>
+__global__ void __launch_bounds__(QCB_FLOW1_THREADS) k_flow_force(Geom g, LinkField<R, NE> W, AlgField<R> F) {
+    const int lt = blockIdx.x & 7;
+    const int64_t h = (int64_t)(blockIdx.x >> 3) * blockDim.x + threadIdx.x;
+    if (h >= g.Vh) return;
+    const int mu = lt >> 1, par = lt & 1;
+    int c[4];
+    site_coords(g, par, (uint32_t)h, c);
+    const int lex = lex_of(g, c);
+    const M3<R> A = staple_rt_rows<R, NE>(g, W, c, lex, par, mu);
+    const M3<R> u = W.load_ro(mu, par, (int)h);
+    F.store(mu, par, (int)h, neg_proj_lie_mul(u, A));
+}
+
+// compute_w1 / w2 / w3: W <- exp(X) W in place (a link's update reads only that link and its
+// forces), X = c F0 (use_f1 = 0, c = a) or a F1 - b F0; FP32 and 12-real links reprojected.
+template <typename R, int NE>
+__global__ void __launch_bounds__(256) k_flow_update(Geom g, LinkField<R, NE> W, AlgField<R> F0, AlgField<R> F1,
+                                                     double a, double b, int use_f1, int reproject) {
+    const int lt = blockIdx.y, mu = lt >> 1, par = lt & 1;
+    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= g.Vh) return;
+    const M3<R> z0 = F0.load(mu, par, (int)h);
+    M3<R> X;
+    if (use_f1) {
+        const M3<R> z1 = F1.load(mu, par, (int)h);
+#pragma unroll
+        for (int k = 0; k < 9; k++) X.e[k] = scl((R)a, z1.e[k]) - scl((R)b, z0.e[k]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 9; k++) X.e[k] = scl((R)a, z0.e[k]);
+    }
+    M3<R> w = mul_nn(exp_su3(X), W.load(mu, par, (int)h));
+    if (reproject) reproject_fp64(w);
+    W.store(mu, par, (int)h, w);
+}
+
+// replace_force_0: F0 <- 8/9 F1 - 17/36 F0.
+template <typename R>
+__global__ void __launch_bounds__(256) k_flow_replace(int64_t Vh, AlgField<R> F0, AlgField<R> F1) {
+    const int lt = blockIdx.y, mu = lt >> 1, par = lt & 1;
+    const int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= Vh) return;
+    const M3<R> z0 = F0.load(mu, par, (int)h), z1 = F1.load(mu, par, (int)h);
+    const R a1 = (R)(8.0 / 9.0), b1 = (R)(17.0 / 36.0);
+    M3<R> zn;
+#pragma unroll
+    for (int k = 0; k < 9; k++) zn.e[k] = scl(a1, z1.e[k]) - scl(b1, z0.e[k]);
+    F0.store(mu, par, (int)h, zn);
+}
+
 // ------------------------------------------------------------------ reductions
 // Block reduction of NV doubles -> partials[blockIdx * NV + k] (warp shuffles, then one
 // warp).  Component k is a maximum when bit k of MAXMASK is set, a sum otherwise.
@@ -1029,6 +1085,36 @@ __global__ void __launch_bounds__(128, QCB_CLOVER_MINB(R)) k_clover_qe(Geom g, L
     for (int64_t h = (int64_t)blockIdx.y * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.y * blockDim.x)
         site_clover_pair<R, NE, 3>(g, U, par, pair, (int)h, v);
     block_sum_store<3>(v, partials, blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// clover_site (observables_mpi.cpp:66-90) at one site, plane (mu, nu), as the 3x3 F (18 doubles), or
+// with mu < 0 local_q_e_clover (:93-112): out[0] = q/(4 pi^2) summed over the three plane pairs,
+// out[1] = e.  One thread.
+template <typename R, int NE>
+__global__ void k_clover_site(Geom g, LinkField<R, NE> U, int par, int h, int mu, int nu, double* out) {
+    if (mu >= 0) {
+        int c[4];
+        site_coords(g, par, (uint32_t)h, c);
+        const int lex = lex_of(g, c);
+        const Steps st = make_steps(g, c);
+        R p;
+        const CloverF<R> F = clover_F(U, st, lex, par, mu, nu, p);
+        const Cx<R> o[3][3] = {{mkc<R>(0, F.d[0]), F.o[0], F.o[1]},
+                               {mkc<R>(-F.o[0].re, F.o[0].im), mkc<R>(0, F.d[1]), F.o[2]},
+                               {mkc<R>(-F.o[1].re, F.o[1].im), mkc<R>(-F.o[2].re, F.o[2].im), mkc<R>(0, F.d[2])}};
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                out[2 * (3 * i + j)] = (double)o[i][j].re;
+                out[2 * (3 * i + j) + 1] = (double)o[i][j].im;
+            }
+    } else {
+        double v[2] = {0.0, 0.0};
+        for (int pair = 0; pair < 3; pair++) site_clover_pair<R, NE, 2>(g, U, par, pair, h, v);
+        out[0] = v[0];
+        out[1] = v[1];
+    }
 }
 
 // Unitarity error ||U U^dag - 1||_F per link (src/bin/test.cpp:58-72): partials (max, sum).

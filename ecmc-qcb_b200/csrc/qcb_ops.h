@@ -38,6 +38,12 @@ struct FmtOps {
                               cudaStream_t s);
     cudaError_t (*flow1)(const Geom& g, const void* win, void* wout, void* z, double eps, int stage, int reproject,
                          cudaStream_t s);
+    cudaError_t (*flow_force)(const Geom& g, const void* w, void* f, cudaStream_t s);
+    cudaError_t (*flow_update)(const Geom& g, void* w, const void* f0, const void* f1, double a, double b, int use_f1,
+                               int reproject, cudaStream_t s);
+    cudaError_t (*flow_replace)(const Geom& g, void* f0, const void* f1, cudaStream_t s);
+    cudaError_t (*clover_site)(const Geom& g, const void* links, int par, int h, int mu, int nu, double* out,
+                               cudaStream_t s);
     cudaError_t (*plaquette)(const Geom& g, const void* links, double* partials, unsigned nbx, cudaStream_t s);
     cudaError_t (*clover)(const Geom& g, const void* links, double* partials, unsigned nbx, cudaStream_t s);
     cudaError_t (*unitarity)(const Geom& g, const void* links, double* partials, unsigned nbx, cudaStream_t s);

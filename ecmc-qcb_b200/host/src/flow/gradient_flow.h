@@ -24,5 +24,17 @@ class GradientFlow {
     ~GradientFlow();
     void copy(const GaugeField& field);
     void rk3_step(mpi::MpiTopology& topo);
+    // The reference's separate passes (gradient_flow.cpp:17-121); force_0 and force_1 live on the
+    // device inside the flow state (the reference's public force_0 / force_1 fields are not exposed).
+    void compute_force(int i);
+    void compute_w1();
+    void compute_w2();
+    void replace_force_0();
+    void compute_w3();
     qcb_flow handle() const { return fl_; }
+
+   private:
+    void run_pass(int pass, const char* what);
+
+   public:
 };

@@ -245,8 +245,52 @@ void GradientFlow::rk3_step(mpi::MpiTopology&) {
     field_c.mark_device_modified();
 }
 
+// The reference's separate passes (gradient_flow.cpp:17-121), one C ABI pass each.
+void GradientFlow::run_pass(int pass, const char* what) {
+    field_c.device();
+    qcb_check(qcb_flow_pass(fl_, pass), what);
+    field_c.mark_device_modified();
+}
+void GradientFlow::compute_force(int i) { run_pass(i == 0 ? QCB_FLOW_FORCE0 : QCB_FLOW_FORCE1, "compute_force"); }
+void GradientFlow::compute_w1() { run_pass(QCB_FLOW_W1, "compute_w1"); }
+void GradientFlow::compute_w2() { run_pass(QCB_FLOW_W2, "compute_w2"); }
+void GradientFlow::replace_force_0() { run_pass(QCB_FLOW_REPLACE_F0, "replace_force_0"); }
+void GradientFlow::compute_w3() { run_pass(QCB_FLOW_W3, "compute_w3"); }
+
 // ====================================================================== observables
+namespace {
+// Lexicographic index of the interior site a halo'd index names (halo sites wrap periodically).
+int64_t interior_lex(const GeometryCB& geo, size_t site) {
+    int c[4];
+    geo.coords(site, c);
+    int64_t lex = 0;
+    for (int d = 3; d >= 0; d--) lex = lex * geo.L_int + (((c[d] - 1) % geo.L_int) + geo.L_int) % geo.L_int;
+    return lex;
+}
+}  // namespace
+
 namespace mpi::observables {
+SU3 clover_site(const GaugeField& field, const GeometryCB& geo, size_t site, int mu, int nu) {
+    double F[18];
+    qcb_check(qcb_clover_site(field.device(), interior_lex(geo, site), mu, nu, F), "clover_site");
+    SU3 r;
+    for (int k = 0; k < 9; k++) r.m[k] = Complex(F[2 * k], F[2 * k + 1]);
+    return r;
+}
+
+// observables_mpi.cpp:51-63: +1 / -1 for even / odd permutations of distinct indices, else 0.
+int levi_civita(int mu, int nu, int rho, int sigma) {
+    if (mu == nu || mu == rho || mu == sigma || nu == rho || nu == sigma || rho == sigma) return 0;
+    const int inv = (mu > nu) + (mu > rho) + (mu > sigma) + (nu > rho) + (nu > sigma) + (rho > sigma);
+    return (inv & 1) ? -1 : 1;
+}
+
+std::pair<double, double> local_q_e_clover(const GaugeField& field, const GeometryCB& geo, size_t site) {
+    double q = 0.0, e = 0.0;
+    qcb_check(qcb_local_qe(field.device(), interior_lex(geo, site), &q, &e), "local_q_e_clover");
+    return {q, e};
+}
+
 double mean_plaquette_local(const GaugeField& field, const GeometryCB& geo) {
     double p = 0;
     qcb_check(qcb_plaquette(field.device(), &p), "plaquette");

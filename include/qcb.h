@@ -129,6 +129,12 @@ int qcb_hb_sweep(qcb_field f, double beta, int n_hits, uint64_t seed, uint32_t s
 int qcb_plaquette(qcb_field f, double* plaq);
 /* topo_q_e_clover_global (src/observables/observables_mpi.cpp:136-156): Q and E = sum(e)/V. */
 int qcb_clover_qe(qcb_field f, double* Q, double* E);
+/* clover_site (src/observables/observables_mpi.cpp:66-90): the clover field strength
+ * F_mu_nu = (C - C^dag)/8 at one site (lexicographic index), 9 complex as 18 doubles, row-major. */
+int qcb_clover_site(qcb_field f, int64_t site, int mu, int nu, double* F_out);
+/* local_q_e_clover (src/observables/observables_mpi.cpp:93-112) at one site: the topological charge
+ * density q (with its 1/(4 pi^2)) and the energy density e. */
+int qcb_local_qe(qcb_field f, int64_t site, double* q, double* e);
 
 /* ------------------------------------------------------------------ Wilson flow */
 /* GradientFlow(double eps, const GaugeField&, const GeometryCB&) (src/flow/gradient_flow.h:11-27,
@@ -146,6 +152,23 @@ int qcb_flow_rk3(qcb_flow fl, int n);
 int qcb_flow_measure(qcb_flow fl, qcb_field src, int n_steps, int n_rk, double* tQE, double* plaq);
 /* The flowed field (GradientFlow::field_c); owned by the flow state. */
 qcb_field qcb_flow_field(qcb_flow fl);
+/* GradientFlow's separate member passes (src/flow/gradient_flow.cpp:17-121, declared
+ * gradient_flow.h:21-25) on the flowed field, for callers that drive them one by one (qcb_flow_rk3
+ * runs the fused stages): force_0 and force_1 are su(3) fields of the flow state.
+ *   QCB_FLOW_FORCE0 / FORCE1   compute_force(0 / 1): F = proj_lie_su3(-U A)
+ *   QCB_FLOW_W1                compute_w1: U <- exp(eps/4 F0) U
+ *   QCB_FLOW_W2                compute_w2: U <- exp(8/9 eps F1 - 17/36 eps F0) U
+ *   QCB_FLOW_REPLACE_F0        replace_force_0: F0 <- 8/9 F1 - 17/36 F0
+ *   QCB_FLOW_W3                compute_w3: U <- exp(3/4 eps F1 - eps F0) U
+ * The reference's rk3_step is FORCE0, W1, FORCE1, W2, REPLACE_F0, FORCE1, W3 (its halo exchanges
+ * are implicit on one GPU).  FP32 and 12-real links are reprojected after each update. */
+#define QCB_FLOW_FORCE0 0
+#define QCB_FLOW_FORCE1 1
+#define QCB_FLOW_W1 2
+#define QCB_FLOW_W2 3
+#define QCB_FLOW_REPLACE_F0 4
+#define QCB_FLOW_W3 5
+int qcb_flow_pass(qcb_flow fl, int pass);
 
 /* ------------------------------------------------------------------ ILDG */
 /* save_ildg_clime (src/io/ildg.cpp:34-136): LIME records "ildg-format" (MB=1, ME=1) and

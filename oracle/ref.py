@@ -61,6 +61,7 @@ def lib():
             "qref_clover_density": (None, [vp, _fp, _fp]),
             "qref_clover_site": (None, [vp, lg, i, i, _dp]),
             "qref_flow_rk3": (None, [vp, d, i]),
+            "qref_flow_passes": (None, [vp, d, C.POINTER(C.c_int), i]),
             "qref_flow_measure": (None, [vp, d, i, i, _fp]),
             "qref_hb_subsweep": (None, [vp, d, i, u64, u32, i, i]),
             "qref_hb_sweep": (None, [vp, d, i, u64, u32]),
@@ -135,6 +136,12 @@ class RefLattice:
 
     def flow_rk3(self, eps: float, n: int = 1) -> None:
         lib().qref_flow_rk3(self._h, float(eps), int(n))
+
+    def flow_passes(self, eps: float, seq) -> None:
+        """GradientFlow's member passes in order (0/1 compute_force(0/1), 2/3/5 compute_w1/2/3,
+        4 replace_force_0); the lattice becomes the flowed field_c."""
+        arr = (C.c_int * len(seq))(*[int(v) for v in seq])
+        lib().qref_flow_passes(self._h, float(eps), arr, len(seq))
 
     def flow_measure(self, eps: float, n_steps: int, n_rk: int) -> np.ndarray:
         out = np.empty(3 * n_steps)

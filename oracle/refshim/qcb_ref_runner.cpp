@@ -184,6 +184,26 @@ void qref_flow_rk3(void* h, double eps, int n) {
     r.field = gf.field_c;
 }
 
+// GradientFlow's member passes in the order given (0 compute_force(0), 1 compute_force(1),
+// 2 compute_w1, 3 compute_w2, 4 replace_force_0, 5 compute_w3), with the halo exchange rk3_step
+// makes after each update (src/flow/gradient_flow.cpp:124-135); the field becomes field_c.
+void qref_flow_passes(void* h, double eps, const int* seq, int n) {
+    RefLattice& r = *static_cast<RefLattice*>(h);
+    GradientFlow gf(eps, r.field, r.geo);
+    for (int k = 0; k < n; k++) {
+        switch (seq[k]) {
+            case 0: gf.compute_force(0); break;
+            case 1: gf.compute_force(1); break;
+            case 2: gf.compute_w1(); break;
+            case 3: gf.compute_w2(); break;
+            case 4: gf.replace_force_0(); break;
+            default: gf.compute_w3(); break;
+        }
+        if (seq[k] == 2 || seq[k] == 3 || seq[k] == 5) mpi::exchange::exchange_halos_cascade(gf.field_c, r.geo, r.topo);
+    }
+    r.field = gf.field_c;
+}
+
 // topo_charge_flowed (src/observables/observables_mpi.cpp:159-186); tQE holds 3*n_steps doubles.
 // The field itself is left unflowed (the reference flows the GradientFlow's copy).
 void qref_flow_measure(void* h, double eps, int n_steps, int n_rk, double* tQE) {

@@ -1,5 +1,7 @@
 // Uses the C++ layer the way the reference's drivers use their own classes and prints what the
 // Python test compares with the oracle.  argv[1]: scratch directory.
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <fstream>
 #include <iomanip>
@@ -97,5 +99,30 @@ int main(int argc, char** argv) {
     for (int k = 0; k < 9; k++) std::cout << " " << A.m[k].real() << " " << A.m[k].imag();
     std::cout << "\n";
     dump(field, geo, dir + "/hit.bin");
+
+    // the reference's separate flow members in rk3_step's order equal one rk3_step
+    GradientFlow gm(0.02, field, geo), gr(0.02, field, geo);
+    gm.compute_force(0);
+    gm.compute_w1();
+    gm.compute_force(1);
+    gm.compute_w2();
+    gm.replace_force_0();
+    gm.compute_force(1);
+    gm.compute_w3();
+    gr.rk3_step(topo);
+    double fd = 0;
+    for (int sx = 0; sx < (int)geo.V_ext; sx++)
+        for (int mu = 0; mu < 4; mu++) {
+            SU3 u = gm.field_c.view_link_const(sx, mu), v = gr.field_c.view_link_const(sx, mu);
+            for (int k = 0; k < 9; k++) fd = std::max(fd, std::abs(u.m[k] - v.m[k]));
+        }
+    std::cout << "members_vs_rk3 " << fd << "\n";
+    SU3 F = mpi::observables::clover_site(field, geo, geo.index(2, 1, 1, 1), 0, 2);
+    auto qe = mpi::observables::local_q_e_clover(field, geo, geo.index(2, 1, 1, 1));
+    std::cout << "clover_site";
+    for (int k = 0; k < 9; k++) std::cout << " " << F.m[k].real() << " " << F.m[k].imag();
+    std::cout << "\nlocal_qe " << qe.first << " " << qe.second << "\n";
+    std::cout << "levi " << mpi::observables::levi_civita(0, 1, 2, 3) << " " << mpi::observables::levi_civita(1, 0, 2, 3)
+              << " " << mpi::observables::levi_civita(0, 0, 2, 3) << "\n";
     return 0;
 }

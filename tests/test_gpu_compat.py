@@ -27,7 +27,8 @@ def run(tmp_path_factory, gpu):
     for line in r.stdout.splitlines():
         parts = line.split()
         if parts and parts[0] in ("hot_key", "plaq_hot", "halo_diff", "staple00", "hb_key", "hb_sweep", "plaq_hb",
-                                  "tqe", "ildg_diff", "plaq_edit", "hit_key", "hit_staple"):
+                                  "tqe", "ildg_diff", "plaq_edit", "hit_key", "hit_staple",
+                                  "members_vs_rk3", "clover_site", "local_qe", "levi"):
             out[parts[0]] = parts[1:]
     return d, out
 
@@ -91,3 +92,17 @@ def test_hit_with_reference_signature(run, orc):
     assert rel_err(H[1, 1], W[1, 1]) < 1e-12
     H[1, 1] = S[1, 1]
     assert np.array_equal(H, S)
+
+
+def test_flow_members_and_site_observables(run, orc):
+    """GradientFlow::compute_force / compute_w1-3 / replace_force_0 in rk3_step's order equal rk3_step;
+    clover_site and local_q_e_clover at one site against the oracle; levi_civita."""
+    d, out = run
+    L = (4, 4, 4, 4)
+    assert float(out["members_vs_rk3"][0]) < 1e-13
+    H = load(d, "hit.bin")  # the field the C++ program measured
+    F = np.array([float(x) for x in out["clover_site"]]).view(np.complex128).reshape(3, 3)
+    assert np.max(np.abs(F.conj().T + F)) < 1e-14  # anti-Hermitian
+    q, e = orc.clover_qe_density(H, L)
+    assert abs(float(out["local_qe"][0]) - q[1]) < 1e-12 and abs(float(out["local_qe"][1]) - e[1]) < 1e-12 * e[1]
+    assert out["levi"] == ["1", "-1", "0"]

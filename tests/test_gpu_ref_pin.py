@@ -225,3 +225,40 @@ def test_copy_then_update_of_source(gpu, orc):
         tol = 1e-12 if fmt[0] == 64 else 1e-6
         assert abs(dst.plaquette() - p0) < tol, fmt
         src.upload(U)
+
+
+@pytest.mark.parametrize("store", STORES)
+def test_flow_member_passes_against_reference(gpu, orc, refc, store):
+    """qcb_flow_pass (GradientFlow::compute_force, compute_w1/2/3, replace_force_0) against the
+    reference's members: the flowed field after each update, and the whole sequence against one
+    fused RK3 step of the CUDA path."""
+    LL, U = _config(orc, 8, 501)
+    f = gpu.GaugeField(LL, 64, store)
+    f.upload(U)
+    fl = gpu.GradientFlow(f, 0.02)
+    seq = [0, 2, 1, 3, 4, 1, 5]
+    for k in (2, 4, 7):
+        r = refc.RefLattice(8, U)
+        r.flow_passes(0.02, seq[:k])
+        fl.copy(f)
+        for p in seq[:k]:
+            fl.run_pass(p)
+        assert rel_err(fl.field.download(), r.get()) < TOL, k
+    fused = gpu.GradientFlow(f, 0.02)
+    fused.rk3_step(1)
+    assert rel_err(fl.field.download(), fused.field.download()) < TOL
+
+
+def test_clover_site_and_local_qe_against_reference(gpu, orc, refc):
+    LL, U = _config(orc, 8, 601)
+    r = refc.RefLattice(8, U)
+    f = gpu.GaugeField(LL, 64, 0)
+    f.upload(U)
+    q_ref, e_ref = r.clover_density()
+    for lex in (0, 1, 77, 4095):
+        for mu, nu in ((0, 1), (2, 3), (3, 1)):
+            assert rel_err(f.clover_site(lex, mu, nu), r.clover_site(lex, mu, nu)) < TOL, (lex, mu, nu)
+        q, e = f.local_qe(lex)
+        assert abs(q - q_ref[lex]) < TOL * max(1.0, abs(q_ref[lex])) and abs(e - e_ref[lex]) < TOL * e_ref[lex]
+    with pytest.raises(gpu.QcbError):
+        f.clover_site(0, 2, 2)

@@ -176,3 +176,11 @@ def test_reference_su3_pieces(orc, refc):
         Z = 0.5 * refc.proj_lie_su3(M)
         for c in (0.005, 0.25, 1.0):
             assert np.max(np.abs(orc.exp_su3(Z, c) - refc.exp_su3_luscher(Z, c))) < 1e-15
+
+
+def test_reference_flow_member_passes(orc, refc):
+    """GradientFlow's member passes in rk3_step's order (with its halo exchanges) are one RK3 step."""
+    LL, U = _config(orc, 6, 71)
+    r = refc.RefLattice(6, U)
+    r.flow_passes(0.02, [0, 2, 1, 3, 4, 1, 5])
+    assert rel_err(r.get(), orc.flow_rk3(U, LL, 0.02, 1)) < TOL
