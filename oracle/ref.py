@@ -68,6 +68,8 @@ def lib():
             "qref_hb_link": (None, [vp, lg, i, d, i, u64, u32, _dp]),
             "qref_projection": (None, [vp]),
             "qref_shift": (None, [vp, C.c_int * 4]),
+            "qref_ildg_write": (i, [vp, C.c_char_p, C.c_char_p]),
+            "qref_ildg_read": (None, [vp, C.c_char_p, C.c_char_p]),
             "qref_exp_su3_luscher": (None, [_dp, d, _dp]),
             "qref_proj_lie_su3": (None, [_dp]),
         }
@@ -164,6 +166,16 @@ class RefLattice:
 
     def shift(self, s) -> None:
         lib().qref_shift(self._h, (C.c_int * 4)(*[int(v) for v in s]))
+
+    def ildg_write(self, directory: str, name: str) -> str:
+        """save_ildg_clime: writes directory/name/name and returns that path."""
+        if lib().qref_ildg_write(self._h, directory.encode(), name.encode()) != 0:
+            raise OSError(f"cannot create {directory}/{name}")
+        return os.path.join(directory, name, name)
+
+    def ildg_read(self, directory: str, name: str) -> None:
+        """read_ildg_clime of directory/name/name (the reference aborts the process on a bad file)."""
+        lib().qref_ildg_read(self._h, directory.encode(), name.encode())
 
 
 def exp_su3_luscher(Z: np.ndarray, coeff: float) -> np.ndarray:

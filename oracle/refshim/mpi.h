@@ -10,8 +10,11 @@
  *   - MPI_Isend/MPI_Irecv queue their buffers and MPI_Wait/MPI_Waitall pair each receive with the
  *     queued send of the same tag and copy it, which is what a periodic one-rank halo exchange
  *     (a rank sending its faces to itself) needs.
- * Anything else (MPI-IO, other collectives) is not declared: a source that needs it does not
- * compile against this header.  Not thread-safe: the reference calls MPI outside its OpenMP
+ *   - MPI-IO as the reference's ILDG code uses it: a file view of one rank's whole lattice (a
+ *     subarray equal to the full array, the only view one rank can have) is one contiguous range at
+ *     the view's displacement, so MPI_File_write_all / read_all are one fwrite / fread there.
+ * Anything else (other collectives, other views) is not declared or refused: a source that needs
+ * it does not compile or aborts.  Not thread-safe: the reference calls MPI outside its OpenMP
  * regions. */
 #ifndef QCB_REFSHIM_MPI_H
 #define QCB_REFSHIM_MPI_H
@@ -45,13 +48,40 @@ typedef struct {
 #define MPI_DOUBLE_COMPLEX 1016
 #define MPI_C_DOUBLE_COMPLEX 1016
 
+#define MPI_OFFSET 8
+#define MPI_DATATYPE_NULL 0
+typedef long long MPI_Offset;
+typedef int MPI_Info;
+#define MPI_INFO_NULL 0
+#define MPI_MODE_RDONLY 2
+#define MPI_MODE_WRONLY 4
+#define MPI_ORDER_C 56
+struct qcb_mpi_file_s {
+    FILE* fp;
+    MPI_Offset disp;
+};
+typedef qcb_mpi_file_s* MPI_File;
+
 #define MPI_SUM 1
 #define MPI_MAX 2
 #define MPI_MIN 3
 #define MPI_LAND 4
 
 namespace qcb_mpi_stub {
-inline size_t type_size(MPI_Datatype t) { return (size_t)(t >= 1000 ? t - 1000 : t); }
+// derived datatypes (ids from kDerived): their size in bytes
+constexpr int kDerived = 1 << 20;
+inline std::vector<size_t>& derived_sizes() {
+    static std::vector<size_t> v;
+    return v;
+}
+inline size_t type_size(MPI_Datatype t) {
+    if (t >= kDerived) return derived_sizes()[(size_t)(t - kDerived)];
+    return (size_t)(t >= 1000 ? t - 1000 : t);
+}
+inline MPI_Datatype new_type(size_t bytes) {
+    derived_sizes().push_back(bytes);
+    return kDerived + (int)derived_sizes().size() - 1;
+}
 
 [[noreturn]] inline void fail(const char* what) {
     std::fprintf(stderr, "one-rank MPI stand-in: %s\n", what);
@@ -156,6 +186,53 @@ inline int MPI_Waitall(int, MPI_Request*, MPI_Status*) {
     return MPI_SUCCESS;
 }
 inline int MPI_Wait(MPI_Request* req, MPI_Status* st) { return MPI_Waitall(1, req, st); }
+inline int MPI_Type_contiguous(int count, MPI_Datatype old, MPI_Datatype* t) {
+    *t = qcb_mpi_stub::new_type((size_t)count * qcb_mpi_stub::type_size(old));
+    return MPI_SUCCESS;
+}
+inline int MPI_Type_commit(MPI_Datatype*) { return MPI_SUCCESS; }
+inline int MPI_Type_free(MPI_Datatype* t) {
+    *t = MPI_DATATYPE_NULL;
+    return MPI_SUCCESS;
+}
+inline int MPI_Type_create_subarray(int ndims, const int* sizes, const int* subsizes, const int* starts, int,
+                                    MPI_Datatype old, MPI_Datatype* t) {
+    size_t n = 1;
+    for (int d = 0; d < ndims; d++) {
+        if (subsizes[d] != sizes[d] || starts[d] != 0) qcb_mpi_stub::fail("a subarray other than the whole array");
+        n *= (size_t)sizes[d];
+    }
+    *t = qcb_mpi_stub::new_type(n * qcb_mpi_stub::type_size(old));
+    return MPI_SUCCESS;
+}
+inline int MPI_File_open(MPI_Comm, const char* path, int amode, MPI_Info, MPI_File* fh) {
+    FILE* fp = std::fopen(path, (amode & MPI_MODE_WRONLY) ? "r+b" : "rb");
+    if (!fp) return 1;
+    *fh = new qcb_mpi_file_s{fp, 0};
+    return MPI_SUCCESS;
+}
+inline int MPI_File_set_view(MPI_File fh, MPI_Offset disp, MPI_Datatype, MPI_Datatype, const char*, MPI_Info) {
+    fh->disp = disp;
+    return MPI_SUCCESS;
+}
+inline int MPI_File_write_all(MPI_File fh, const void* buf, int count, MPI_Datatype t, MPI_Status*) {
+    const size_t n = (size_t)count * qcb_mpi_stub::type_size(t);
+    if (fseeko(fh->fp, (off_t)fh->disp, SEEK_SET) || std::fwrite(buf, 1, n, fh->fp) != n)
+        qcb_mpi_stub::fail("MPI_File_write_all");
+    return MPI_SUCCESS;
+}
+inline int MPI_File_read_all(MPI_File fh, void* buf, int count, MPI_Datatype t, MPI_Status*) {
+    const size_t n = (size_t)count * qcb_mpi_stub::type_size(t);
+    if (fseeko(fh->fp, (off_t)fh->disp, SEEK_SET) || std::fread(buf, 1, n, fh->fp) != n)
+        qcb_mpi_stub::fail("MPI_File_read_all");
+    return MPI_SUCCESS;
+}
+inline int MPI_File_close(MPI_File* fh) {
+    std::fclose((*fh)->fp);
+    delete *fh;
+    *fh = nullptr;
+    return MPI_SUCCESS;
+}
 inline int MPI_Abort(MPI_Comm, int code) {
     std::fprintf(stderr, "MPI_Abort(%d)\n", code);
     std::exit(code);

@@ -404,6 +404,10 @@ public:
         return p_[Plain::offset(i, j)];
     }
     Scalar operator()(Index i, Index j) const { return p_[Plain::offset((int)i, (int)j)]; }
+    template <bool C = IsConst, std::enable_if_t<!C, int> = 0>
+    Scalar& operator()(Index i, Index j) {
+        return p_[Plain::offset((int)i, (int)j)];
+    }
     Pointer data() const { return p_; }
 
 private:

@@ -17,6 +17,7 @@
 // CUDA path; the update arithmetic is the reference's.
 #include <cstdint>
 #include <cstring>
+#include <filesystem>
 #include <iomanip>
 #include <iostream>
 #include <sstream>
@@ -27,6 +28,7 @@
 #include "gauge/GaugeField.h"
 #include "geometry/GeometryCB.h"
 #include "heatbath/heatbath_mpi.h"
+#include "io/ildg.h"
 #include "io/io.h"
 #include "mpi/HalosExchange.h"
 #include "mpi/HalosShift.h"
@@ -254,6 +256,22 @@ void qref_shift(void* h, const int s[4]) {
     RefLattice& r = *static_cast<RefLattice*>(h);
     mpi::shift::shift_field(r.field, r.geo, r.hs, r.topo, s);
     r.halos();
+}
+
+// save_ildg_clime / read_ildg_clime (src/io/ildg.cpp:34-237): the file is dir/name/name, as the
+// reference lays it out; the writer's run directory dir/name is created first (the reference's
+// driver has made it by the time it saves).
+int qref_ildg_write(void* h, const char* dir, const char* name) {
+    RefLattice& r = *static_cast<RefLattice*>(h);
+    std::error_code ec;
+    std::filesystem::create_directories(std::filesystem::path(dir) / name, ec);
+    if (ec) return -1;
+    quiet([&] { save_ildg_clime(name, dir, r.field, r.geo, r.topo); });
+    return 0;
+}
+void qref_ildg_read(void* h, const char* dir, const char* name) {
+    RefLattice& r = *static_cast<RefLattice*>(h);
+    read_ildg_clime(name, dir, r.field, r.geo, r.topo);
 }
 
 // exp_su3_luscher (src/su3/utils.cpp:145-193) and proj_lie_su3 (:130-134) on one matrix.

@@ -262,3 +262,31 @@ def test_clover_site_and_local_qe_against_reference(gpu, orc, refc):
         assert abs(q - q_ref[lex]) < TOL * max(1.0, abs(q_ref[lex])) and abs(e - e_ref[lex]) < TOL * e_ref[lex]
     with pytest.raises(gpu.QcbError):
         f.clover_site(0, 2, 2)
+
+
+@pytest.mark.parametrize("store", STORES)
+def test_ildg_files_match_reference_writer(gpu, orc, refc, tmp_path, store):
+    """qcb_ildg_write produces the reference's save_ildg_clime file byte for byte (LIME records,
+    flags, XML text, big-endian payload); each side reads the other's file back exactly, and the
+    reference reads a file that carries the optional SciDAC checksum record."""
+    LL, U = _config(orc, 4, 701)
+    r = refc.RefLattice(4, U)
+    ref_path = r.ildg_write(str(tmp_path), "ref")
+    f = gpu.GaugeField(LL, 64, store)
+    f.upload(U)
+    os.makedirs(str(tmp_path / "ours"), exist_ok=True)
+    ours = str(tmp_path / "ours" / "ours")
+    f.save_ildg(ours)
+    U_dev = f.download()
+    if store == 0:
+        assert open(ours, "rb").read() == open(ref_path, "rb").read()
+    g = gpu.GaugeField(LL, 64, 0)
+    g.read_ildg(ref_path)
+    assert np.array_equal(g.download(), U)
+    s = refc.RefLattice(4)
+    s.ildg_read(str(tmp_path), "ours")
+    assert np.array_equal(s.get(), U_dev)
+    os.makedirs(str(tmp_path / "sum"), exist_ok=True)
+    f.save_ildg(str(tmp_path / "sum" / "sum"), scidac_checksum=True)
+    s.ildg_read(str(tmp_path), "sum")
+    assert np.array_equal(s.get(), U_dev)

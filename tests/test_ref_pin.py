@@ -184,3 +184,25 @@ def test_reference_flow_member_passes(orc, refc):
     r = refc.RefLattice(6, U)
     r.flow_passes(0.02, [0, 2, 1, 3, 4, 1, 5])
     assert rel_err(r.get(), orc.flow_rk3(U, LL, 0.02, 1)) < TOL
+
+
+def test_reference_ildg_round_trip(orc, refc, tmp_path):
+    """The reference's own save_ildg_clime / read_ildg_clime (LIME framing by the project's
+    stand-in for c-lime): a written configuration reads back exactly; the file has the reference's
+    two records (ildg-format MB=1 ME=1, ildg-binary-data MB=0 ME=1) and big-endian payload."""
+    import struct
+
+    LL, U = _config(orc, 4, 81)
+    r = refc.RefLattice(4, U)
+    path = r.ildg_write(str(tmp_path), "cfg")
+    b = open(path, "rb").read()
+    magic, ver, flags, n = struct.unpack(">IHHQ", b[:16])
+    assert (magic, ver, flags >> 14) == (0x456789AB, 1, 3) and b[16:27] == b"ildg-format"
+    off = 144 + ((n + 7) & ~7)
+    magic, ver, flags, n2 = struct.unpack(">IHHQ", b[off:off + 16])
+    assert flags >> 14 == 1 and b[off + 16:off + 32] == b"ildg-binary-data" and n2 == 256 * 72 * 8
+    payload = np.frombuffer(b[off + 144:off + 144 + n2], dtype=">f8").astype(np.float64)
+    assert np.array_equal(payload.view(np.complex128).reshape(U.shape), U)
+    s = refc.RefLattice(4)
+    s.ildg_read(str(tmp_path), "cfg")
+    assert np.array_equal(s.get(), U)
