@@ -935,11 +935,11 @@ int qcb_flow_pass(qcb_flow fl, int pass) {
             });
         case QCB_FLOW_W1:
             return launch(f, QCB_K_FLOW, [&] {
-                return o.flow_update(f->g, f->links, fl->z, nullptr, 0.25 * e, 0.0, 0, rep, f->stream);
+                return o.flow_update(f->g, f->links, fl->z, nullptr, 0.25 * e, 0.0, 0, 0, f->stream);
             });
         case QCB_FLOW_W2:
             return launch(f, QCB_K_FLOW, [&] {
-                return o.flow_update(f->g, f->links, fl->z, fl->f1, (8.0 / 9.0) * e, (17.0 / 36.0) * e, 1, rep,
+                return o.flow_update(f->g, f->links, fl->z, fl->f1, (8.0 / 9.0) * e, (17.0 / 36.0) * e, 1, 0,
                                      f->stream);
             });
         case QCB_FLOW_REPLACE_F0:

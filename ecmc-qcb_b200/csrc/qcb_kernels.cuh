@@ -732,7 +732,9 @@ __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>&
     }
     M3<R> E = exp_su3(X);
     M3<R> w = mul_nn(E, u);
-    if (reproject) reproject_fp64(w);
+    // FP32 and 12-real links: one FP64 reprojection per RK3 step, after its last stage (after every
+    // stage the FP32 stage took 4-5% longer, with the same flowed Q and E against FP64).
+    if (STAGE == 3 && reproject) reproject_fp64(w);
     Wout.store(mu, par, h, w);
 }
 
@@ -767,7 +769,8 @@ __global__ void __launch_bounds__(QCB_FLOW1_THREADS) k_flow_force(Geom g, LinkFi
 }
 
 // compute_w1 / w2 / w3: W <- exp(X) W in place (a link's update reads only that link and its
-// forces), X = c F0 (use_f1 = 0, c = a) or a F1 - b F0; FP32 and 12-real links reprojected.
+// forces), X = c F0 (use_f1 = 0, c = a) or a F1 - b F0; FP32 and 12-real links reprojected after
+// compute_w3 (the caller passes reproject = 0 for w1 and w2), as after the fused third stage.
 template <typename R, int NE>
 __global__ void __launch_bounds__(256) k_flow_update(Geom g, LinkField<R, NE> W, AlgField<R> F0, AlgField<R> F1,
                                                      double a, double b, int use_f1, int reproject) {

@@ -38,7 +38,8 @@ extern "C" {
 #define QCB_PREC_F32 32
 #define QCB_STORE_18 0 /* full 3x3 complex matrix (18 reals) */
 #define QCB_STORE_12 1 /* first two rows (12 reals), third rebuilt in registers; links in this
-                          * storage are reprojected to SU(3) in FP64 after every update */
+                          * storage (and FP32 links) are reprojected to SU(3) in FP64 after every
+                          * heatbath update and every RK3 step */
 
 typedef struct qcb_field_s* qcb_field;
 typedef struct qcb_flow_s* qcb_flow;
@@ -161,7 +162,8 @@ qcb_field qcb_flow_field(qcb_flow fl);
  *   QCB_FLOW_REPLACE_F0        replace_force_0: F0 <- 8/9 F1 - 17/36 F0
  *   QCB_FLOW_W3                compute_w3: U <- exp(3/4 eps F1 - eps F0) U
  * The reference's rk3_step is FORCE0, W1, FORCE1, W2, REPLACE_F0, FORCE1, W3 (its halo exchanges
- * are implicit on one GPU).  FP32 and 12-real links are reprojected after each update. */
+ * are implicit on one GPU).  FP32 and 12-real links are reprojected after QCB_FLOW_W3, as after a
+ * fused RK3 step. */
 #define QCB_FLOW_FORCE0 0
 #define QCB_FLOW_FORCE1 1
 #define QCB_FLOW_W1 2

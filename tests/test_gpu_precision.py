@@ -31,7 +31,7 @@ def test_fp32_flow_against_fp64(gpu, thermalised, store):
     assert np.max(np.abs(t32[:, 2] - t64[:, 2]) / t64[:, 2]) < DE_REL_MAX
     assert np.max(np.abs(p32 - p64)) < DP_MAX
     mx, _ = fl.field.unitarity()
-    assert mx < 1e-6  # reprojected in FP64 after every stage, stored in FP32
+    assert mx < 1e-6  # reprojected in FP64 after every RK3 step, stored in FP32
 
 
 def test_fp32_heatbath_stays_on_su3(gpu):
