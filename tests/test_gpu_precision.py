@@ -34,6 +34,23 @@ def test_fp32_flow_against_fp64(gpu, thermalised, store):
     assert mx < 1e-6  # reprojected in FP64 after every RK3 step, stored in FP32
 
 
+@pytest.mark.parametrize("store", [0, 1])
+def test_fp32_member_passes_equal_fused_step(gpu, thermalised, store):
+    """GradientFlow's separate passes (compute_force, compute_w1/2/3, replace_force_0) on FP32 links,
+    reprojected once after compute_w3 as the fused step is after its third stage, give the fused
+    RK3 step's links to FP32 rounding."""
+    fused = gpu.GradientFlow(thermalised, 0.02, prec=32, store=store)
+    fused.rk3_step(1)
+    fl = gpu.GradientFlow(thermalised, 0.02, prec=32, store=store)
+    for p in (fl.FORCE0, fl.W1, fl.FORCE1, fl.W2, fl.REPLACE_F0, fl.FORCE1, fl.W3):
+        fl.run_pass(p)
+    assert np.max(np.abs(fl.field.download() - fused.field.download())) < 1e-5
+    mx, _ = fl.field.unitarity()
+    assert mx < 1e-6
+    fl.close()
+    fused.close()
+
+
 def test_fp32_heatbath_stays_on_su3(gpu):
     f = gpu.GaugeField((8, 8, 8, 8), 32, 0)
     f.hot_start(3)
