@@ -704,8 +704,10 @@ def run_ours(args, rank: int, world: int, local: int):
         return
 
     # ---------------- device-resident heatbath: warm-up, then K timed sweeps
+    # (--only hb --hb-hits n profiles the kernel at another N_hits; every bench line uses N_HITS)
+    nh = args.hb_hits if args.only == "hb" else N_HITS
     for i in range(args.warmup):
-        f.hb_sweep(BETA, N_HITS, SEED_HB, i)
+        f.hb_sweep(BETA, nh, SEED_HB, i)
     f.sync()
     barrier(world)
     f.timing(True)
@@ -715,7 +717,7 @@ def run_ours(args, rank: int, world: int, local: int):
         torch.cuda.synchronize()
         e0.record(stream)
         for i in range(args.steps):
-            f.hb_sweep(BETA, N_HITS, SEED_HB, args.warmup + i)
+            f.hb_sweep(BETA, nh, SEED_HB, args.warmup + i)
         e1.record(stream)
         e1.synchronize()
         torch.cuda.synchronize()
@@ -861,6 +863,8 @@ def main():
     ap.add_argument("--parts", default="all", choices=["all", "core"],
                     help="core: skip the batch and serving sections")
     ap.add_argument("--serve-requests", type=int, default=32)
+    ap.add_argument("--hb-hits", type=int, default=N_HITS,
+                    help="N_hits of the heatbath with --only hb (ncu captures at another N_hits)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
