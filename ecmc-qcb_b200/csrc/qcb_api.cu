@@ -9,12 +9,19 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
 #include <new>
 #include <string>
 
 #include "qcb_internal.h"
 #include "qcb_ops.h"
+
+// Measured flows take each measurement from the following RK3 step's stage 1 (clover halves) rather
+// than a separate clover pass; 0 keeps the clover pass for every measurement.
+#ifndef QCB_FLOW_FUSED_MEAS
+#define QCB_FLOW_FUSED_MEAS 1
+#endif
 
 using namespace qcb;
 
@@ -208,6 +215,34 @@ int flow_step(qcb_flow_s* fl) {
     return QCB_OK;
 }
 
+// One RK3 step that also measures its input configuration: stage 1 writes the clover halves
+// (k_flow_stage1_meas; its links are those of the plain stage 1), their per-site sum gives
+// (q, e, plaquette sum) in dst[0..2], then stages 2 and 3 as in flow_step.  The standalone clover
+// pass forms every leaf with three products a plane and site; here the force's own staples give
+// the clover with two products a plane and link.
+int flow_step_meas(qcb_flow_s* fl, double* dst) {
+    qcb_field_s* f = fl->fld;
+    RET(ensure_alt(f));
+    const int rep = needs_reproject(f->prec, f->store);
+    RET(launch(f, QCB_K_FLOW, [&] {
+        return fmt_ops(f->fmt).flow1_meas(f->g, f->links, f->alt, fl->z, fl->eps, rep, fl->halves, f->stream);
+    }));
+    const unsigned nb = halves_blocks(f->g.Vh);
+    RET(launch(f, QCB_K_CLOVER,
+               [&] { return fmt_ops(f->fmt).clover_halves(f->g, fl->halves, f->partials, nb, f->stream); }));
+    RET(finalize(f, (int)nb, 3, 0u, dst));
+    for (int stage = 2; stage <= 3; stage++) {
+        void* win = (stage == 2) ? f->alt : f->links;
+        void* wout = (stage == 2) ? f->links : f->alt;
+        RET(launch(f, QCB_K_FLOW,
+                   [&] { return fmt_ops(f->fmt).flow1(f->g, win, wout, fl->z, fl->eps, stage, rep, f->stream); }));
+    }
+    void* t = f->links;
+    f->links = f->alt;
+    f->alt = t;
+    return QCB_OK;
+}
+
 // ------------------------------------------------------------------ flow step graphs
 // Without per-launch timing, the flow's repeated launch sequences are captured once as CUDA graphs
 // and replayed: two RK3 steps (six stage launches; the ping-pong buffers are back in place after
@@ -292,17 +327,23 @@ int flow_graph_run(qcb_flow_s* fl, int kind, int n_rk) {
     return QCB_OK;
 }
 
-// One measurement of the flowed field -- clover pass (q, e and the plaquette sum) into the fixed
-// slot, copied to the next row of the measurement buffer -- followed by n_rk RK3 steps.
+// One measurement of the flowed field -- (q, e and the plaquette sum) into the fixed slot, copied to
+// the next row of the measurement buffer -- followed by n_rk RK3 steps.  With a step to follow
+// (and the halves buffer in place) the measurement comes from that step's stage 1; the last
+// measurement of a run uses the clover pass.
 int meas_block(qcb_flow_s* fl, int n_rk) {
     qcb_field_s* f = fl->fld;
     double* slot = f->d_res + kMeasSlot;
-    RET(enq_clover(f, slot));
+    const bool fused = n_rk > 0 && fl->halves;
+    if (fused)
+        RET(flow_step_meas(fl, slot));
+    else
+        RET(enq_clover(f, slot));
     RET(launch(f, QCB_K_OTHER, [&] {
         k_meas_scatter<<<1, 1, 0, f->stream>>>(slot, fl->d_meas, fl->d_count);
         return cudaGetLastError();
     }));
-    for (int k = 0; k < n_rk; k++) RET(flow_step(fl));
+    for (int k = fused ? 1 : 0; k < n_rk; k++) RET(flow_step(fl));
     return QCB_OK;
 }
 
@@ -856,6 +897,7 @@ int qcb_flow_destroy(qcb_flow fl) {
     if (fl->f1) cudaFree(fl->f1);
     if (fl->d_meas) cudaFree(fl->d_meas);
     if (fl->d_count) cudaFree(fl->d_count);
+    if (fl->halves) cudaFree(fl->halves);
     if (fl->z) cudaFree(fl->z);
     qcb_field_destroy(fl->fld);
     delete fl;
@@ -891,7 +933,11 @@ int qcb_flow_measure(qcb_flow fl, qcb_field src, int n_steps, int n_rk, double* 
     }
     if (!fl->d_count) CK(cudaMalloc(&fl->d_count, sizeof(int)));
     RET(ensure_alt(f));
-    RET(ensure_partials(f, (size_t)clover_blocks(f->g.Vh) * 18));
+    RET(ensure_partials(f, std::max((size_t)clover_blocks(f->g.Vh) * 18, (size_t)halves_blocks(f->g.Vh) * 3)));
+#if QCB_FLOW_FUSED_MEAS
+    // the clover halves of the measuring stage 1, allocated before any graph capture
+    if (n_rk > 0 && n_steps > 1 && !fl->halves) CK(cudaMalloc(&fl->halves, halves_bytes(f->fmt, f->g.Vh)));
+#endif
     CK(cudaMemsetAsync(fl->d_count, 0, sizeof(int), f->stream));
     const bool graphs = graphs_ok(f) && n_rk > 0;
     for (int s = 0; s < n_steps; s++) {

@@ -121,6 +121,23 @@ struct FmtImpl {
         return cudaGetLastError();
     }
 
+    static cudaError_t flow1_meas(const Geom& g, const void* win, void* wout, void* z, double eps, int rep,
+                                  void* hbuf, cudaStream_t s) {
+        const unsigned nb = 8u * (unsigned)((g.Vh + QCB_FLOW1_THREADS - 1) / QCB_FLOW1_THREADS);
+        AlgField<R> za;
+        za.p = (typename AlgField<R>::C2*)z;
+        za.Vh = g.Vh;
+        const HalfClovers<R> H{(R*)hbuf, 2 * g.Vh};
+        k_flow_stage1_meas<R, NE><<<nb, QCB_FLOW1_THREADS, 0, s>>>(g, view(win, g.Vh), view(wout, g.Vh), za, eps,
+                                                                   rep, H);
+        return cudaGetLastError();
+    }
+    static cudaError_t clover_halves(const Geom& g, const void* hbuf, double* partials, unsigned nb, cudaStream_t s) {
+        const HalfClovers<R> H{(R*)hbuf, 2 * g.Vh};
+        k_clover_halves<R><<<nb, 128, 0, s>>>(g, H, partials);
+        return cudaGetLastError();
+    }
+
     static AlgField<R> alg(const void* p, int64_t Vh) {
         AlgField<R> z;
         z.p = (typename AlgField<R>::C2*)p;
@@ -218,6 +235,8 @@ struct FmtImpl {
         o.hb_one = &hb_one;
         o.probe_link = &probe_link;
         o.flow1 = &flow1;
+        o.flow1_meas = &flow1_meas;
+        o.clover_halves = &clover_halves;
         o.flow_force = &flow_force;
         o.flow_update = &flow_update;
         o.flow_replace = &flow_replace;

@@ -20,6 +20,12 @@ inline size_t fmt_cbytes(int fmt) { return (fmt & 2) ? sizeof(float2) : sizeof(d
 inline size_t tiled_sites(int64_t Vh) { return (size_t)((Vh + 31) / 32) * 32; }
 inline size_t link_bytes(int fmt, int64_t Vh) { return (size_t)8 * fmt_ne(fmt) * tiled_sites(Vh) * fmt_cbytes(fmt); }
 inline size_t alg_bytes(int fmt, int64_t Vh) { return (size_t)8 * 4 * tiled_sites(Vh) * fmt_cbytes(fmt); }
+// Device bytes of the clover halves a measuring stage 1 writes: per site 6 planes x 2 halves x 9
+// reals and 6 plaquette traces (HalfClovers in qcb_kernels.cuh), in the link precision.
+constexpr int kHalfCloverReals = 6 * 2 * 9 + 6;
+inline size_t halves_bytes(int fmt, int64_t Vh) { return (size_t)kHalfCloverReals * 2 * Vh * (fmt_cbytes(fmt) / 2); }
+// Blocks of the per-site sum of the clover halves (one thread per site, 128 a block).
+inline unsigned halves_blocks(int64_t Vh) { return (unsigned)((2 * Vh + 127) / 128); }
 
 // Lattice extents every entry point accepts: even, >= 2, at most 2^30 sites.  The running volume
 // is checked after each factor (and every factor is at most 2^30), so no product overflows.
@@ -109,6 +115,7 @@ struct qcb_flow_s {
     double* d_meas = nullptr;     // measurement rows (t-independent: q, e, plaquette sums) of qcb_flow_measure
     size_t meas_cap = 0;          // rows
     int* d_count = nullptr;       // device row counter of the measurement graphs
+    void* halves = nullptr;       // clover halves of a measuring stage 1 (halves_bytes), at first use
     FlowGraph graphs[4];
     uint64_t graph_clock = 0;
 };

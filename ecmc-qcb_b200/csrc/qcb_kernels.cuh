@@ -210,6 +210,174 @@ __device__ __forceinline__ M3<R> staple_rt_rows(const Geom& g, const LinkField<R
     return A;
 }
 
+// ------------------------------------------------------------------ clover halves from the force's staples
+// The clover sum C of plane (mu, nu) at site x (clover_site, observables_mpi.cpp:66-90) enters the
+// observables only through acc(C): o_ij = C_ij - conj(C_ji) (i < j) and d_i = Im C_ii, which is
+// linear and odd under the adjoint.  With D(y) = S_f(y) - S_b(y), the forward minus the backward
+// staple of link (y, mu) in plane nu (the two terms compute_staple sums for that plane),
+//   leaves 1 + 4 of x:  acc(U_mu(x) D(x)),      leaves 2 + 3 of x:  acc(D(x - mu) U_mu(x - mu)),
+// since leaf 1 = U_mu(x) S_f(x), leaf 4 = (U_mu(x) S_b(x))^dag, leaf 2 = (S_f(x-mu) U_mu(x-mu))^dag
+// and leaf 3 = S_b(x-mu) U_mu(x-mu) up to the adjoint's sign.  Stage 1 of an RK3 step forms S_f and
+// S_b of every link for its force, so with two more products a plane (U D and D U) it yields the
+// clover of its input configuration: the link (y, mu) writes the half for leaves 1 + 4 of y and the
+// half for leaves 2 + 3 of y + mu, and k_clover_halves adds the two halves of each site.  From the
+// nu links, plane (mu, nu) appears with the orientation reversed and both halves change sign.
+// Each plane is handled by the links of one direction (two planes at most a direction):
+//   plane 01 -> 0, 02 -> 2, 03 -> 3, 12 -> 1, 13 -> 3, 23 -> 2.
+__host__ __device__ __forceinline__ int plane_index(int a, int b) {  // a < b: 01 02 03 12 13 23
+    return a == 0 ? b - 1 : (a == 1 ? b + 1 : 5);
+}
+__host__ __device__ __forceinline__ int plane_owner(int p) { return (0x231320 >> (4 * p)) & 0xF; }
+
+// The halves of every (plane, site): nine reals (o01, o02, o12 as re/im pairs, then d0, d1, d2) for
+// half 0 (leaves 1 + 4) and half 1 (leaves 2 + 3) of each plane, and Re Tr of leaf 1 (the plaquette
+// trace) of each plane; reals at p[k * V + site], site = parity * Vh + h.
+template <typename R>
+struct HalfClovers {
+    R* p;
+    int64_t V;
+    __device__ __forceinline__ void put_half(int plane, int half, int64_t site, const R v[9], R sign) const {
+#pragma unroll
+        for (int k = 0; k < 9; k++) p[(int64_t)((plane * 2 + half) * 9 + k) * V + site] = sign * v[k];
+    }
+    __device__ __forceinline__ void put_plaq(int plane, int64_t site, R tr) const {
+        p[(int64_t)(108 + plane) * V + site] = tr;
+    }
+};
+
+// acc(A B) for full 3x3 A, B: the six off-diagonal entries of A B and the imaginary parts of its
+// diagonal, in the order of HalfClovers.
+template <typename R>
+__device__ __forceinline__ void acc_product(const M3<R>& A, const M3<R>& B, R out[9]) {
+    Cx<R> m[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            if (i == j) continue;
+            m[i][j] = mkc<R>(0, 0);
+#pragma unroll
+            for (int q = 0; q < 3; q++) cmac(m[i][j], A(i, q), B(q, j));
+        }
+    const int I[3] = {0, 0, 1}, J[3] = {1, 2, 2};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        out[2 * k] = m[I[k]][J[k]].re - m[J[k]][I[k]].re;
+        out[2 * k + 1] = m[I[k]][J[k]].im + m[J[k]][I[k]].im;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        R im = R(0);
+#pragma unroll
+        for (int q = 0; q < 3; q++) im = fma(A(i, q).re, B(q, i).im, fma(A(i, q).im, B(q, i).re, im));
+        out[6 + i] = im;
+    }
+}
+
+// staple_rt_rows, and for the planes this direction handles the two clover halves and the plaquette
+// trace of the link's site (see above).  u is the link U_mu(x) itself.
+template <typename R, int NE>
+__device__ __forceinline__ M3<R> staple_rt_rows_meas(const Geom& g, const LinkField<R, NE>& U, const int c[4],
+                                                     int lex, int par, int mu, const M3<R>& u,
+                                                     const HalfClovers<R>& H) {
+    M3<R> A;
+    set_zero(A);
+    const int opp = par ^ 1;
+    const Steps st = make_steps(g, c);
+    const int xmu = lex + sel4(st.up, mu);
+    const int64_t site = (int64_t)par * g.Vh + (lex >> 1), site_up = (int64_t)opp * g.Vh + (xmu >> 1);
+#pragma unroll 1
+    for (int k = 0; k < 3; k++) {
+        const int nu = k < mu ? k : k + 1;
+        const int plane = mu < nu ? plane_index(mu, nu) : plane_index(nu, mu);
+        const bool owned = plane_owner(plane) == mu;
+        const int dnu = sel4(st.dn, nu);
+        const int xnu = lex + sel4(st.up, nu);
+        const int xmnu = lex + dnu;
+        const int xmumnu = xmu + dnu;
+        M3<R> Sf;
+        {
+            const M3<R> a = U.load_ro(nu, opp, xmu >> 1);
+            const M3<R> b = U.load_ro(mu, opp, xnu >> 1);
+            Cx<R> t[2][3];
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    t[i][j] = mkc<R>(0, 0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) cmac_nc(t[i][j], a(i, q), b(j, q));
+                }
+            const M3<R> d = U.load_ro(nu, par, lex >> 1);
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    Cx<R> v = mkc<R>(0, 0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) cmac_nc(v, t[i][q], d(j, q));
+                    Sf(i, j) = v;
+                    A(i, j) = A(i, j) + v;
+                }
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+                Sf(2, j) = conj_cross(Sf(0, j1), Sf(1, j2), Sf(0, j2), Sf(1, j1));
+                A(2, j) = A(2, j) + Sf(2, j);
+            }
+        }
+        M3<R> Sb;
+        {
+            const M3<R> v1 = U.load_ro(mu, opp, xmnu >> 1);
+            const M3<R> v0 = U.load_ro(nu, par, xmumnu >> 1);
+            Cx<R> t[3][2];
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    t[i][j] = mkc<R>(0, 0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) cmac(t[i][j], v1(i, q), v0(q, j));
+                }
+            const M3<R> v2 = U.load_ro(nu, opp, xmnu >> 1);
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    Cx<R> v = mkc<R>(0, 0);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) cmac_cn(v, t[q][i], v2(q, j));
+                    Sb(i, j) = v;
+                    A(i, j) = A(i, j) + v;
+                }
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+                Sb(2, j) = conj_cross(Sb(0, j1), Sb(1, j2), Sb(0, j2), Sb(1, j1));
+                A(2, j) = A(2, j) + Sb(2, j);
+            }
+        }
+        if (owned) {
+            R tr = R(0);
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int q = 0; q < 3; q++) tr = fma(u(i, q).re, Sf(q, i).re, fma(-u(i, q).im, Sf(q, i).im, tr));
+            H.put_plaq(plane, site, tr);
+            M3<R> D;
+#pragma unroll
+            for (int e = 0; e < 9; e++) D.e[e] = Sf.e[e] - Sb.e[e];
+            const R sign = mu < nu ? R(1) : R(-1);
+            R v[9];
+            acc_product(u, D, v);
+            H.put_half(plane, 0, site, v, sign);
+            acc_product(D, u, v);
+            H.put_half(plane, 1, site_up, v, sign);
+        }
+    }
+    return A;
+}
+
 // -proj_lie(u A) (compute_force, gradient_flow.cpp:17-37) forming only the entries the
 // projection reads: the six off-diagonal entries of u A and the imaginary parts of its diagonal.
 template <typename R>
@@ -273,6 +441,10 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
 #endif
 #ifndef QCB_FLOW1_MINB
 #define QCB_FLOW1_MINB(R) QCB_FLOW_MINB(R)
+#endif
+// stage 1 with the clover halves: the forward staple is held until the backward one is formed
+#ifndef QCB_FLOW_MEAS_MINB
+#define QCB_FLOW_MEAS_MINB(R) (sizeof(R) == 8 ? 2 : 4)
 #endif
 #ifndef QCB_FLOW_RTMU
 #define QCB_FLOW_RTMU 1
@@ -677,15 +849,22 @@ __global__ void k_hb_one(Geom g, LinkField<R, NE> U, int par, int h, double c_al
 //   stage 3: W' = exp(3/4 eps F - eps Z) W                          compute_w3
 // The whole field of forces is never materialised: Win is read-only for the launch and W'
 // goes to a second buffer (ping-pong), which is what makes force and update one pass.
-template <typename R, int NE, int STAGE>
+template <typename R, int NE, int STAGE, bool MEAS = false>
 __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>& Win, const LinkField<R, NE>& Wout,
                                           const AlgField<R>& Z, double eps, int mu, int par, int h,
-                                          int reproject) {
+                                          int reproject, const HalfClovers<R>& H = HalfClovers<R>{}) {
+    static_assert(!MEAS || (STAGE == 1 && (sizeof(R) == 4 || QCB_FLOW64_ROWS)),
+                  "the clover halves come from stage 1's two-row staples");
     int c[4];
     site_coords(g, par, (uint32_t)h, c);
     const int lex = lex_of(g, c);
     M3<R> F, u;
-    if constexpr (sizeof(R) == 4 || QCB_FLOW64_ROWS) {
+    if constexpr (MEAS) {
+        // the same staple and force, with the clover halves of the input configuration
+        u = Win.load_ro(mu, par, h);
+        const M3<R> A = staple_rt_rows_meas<R, NE>(g, Win, c, lex, par, mu, u, H);
+        F = neg_proj_lie_mul(u, A);
+    } else if constexpr (sizeof(R) == 4 || QCB_FLOW64_ROWS) {
         // two-row staple products and the projection's entries only
         const M3<R> A = staple_rt_rows<R, NE>(g, Win, c, lex, par, mu);
         u = Win.load_ro(mu, par, h);
@@ -747,6 +926,19 @@ __global__ void __launch_bounds__(QCB_FLOW1_THREADS, QCB_FLOW1_MINB(R))
     const int64_t h = (int64_t)(blockIdx.x >> 3) * blockDim.x + threadIdx.x;
     if (h >= g.Vh) return;
     flow_link<R, NE, STAGE>(g, Win, Wout, Z, eps, lt >> 1, lt & 1, (int)h, reproject);
+}
+
+// Stage 1 that also writes the clover halves of its input configuration (the measurement of a
+// measured flow step; k_clover_halves completes it).  The links it writes are those of
+// k_flow_stage<R, NE, 1>, bit for bit.
+template <typename R, int NE>
+__global__ void __launch_bounds__(QCB_FLOW1_THREADS, QCB_FLOW_MEAS_MINB(R))
+    k_flow_stage1_meas(Geom g, LinkField<R, NE> Win, LinkField<R, NE> Wout, AlgField<R> Z, double eps, int reproject,
+                       HalfClovers<R> H) {
+    const int lt = blockIdx.x & 7;
+    const int64_t h = (int64_t)(blockIdx.x >> 3) * blockDim.x + threadIdx.x;
+    if (h >= g.Vh) return;
+    flow_link<R, NE, 1, true>(g, Win, Wout, Z, eps, lt >> 1, lt & 1, (int)h, reproject, H);
 }
 
 // ------------------------------------------------------------------ the reference's separate flow passes
@@ -1109,6 +1301,41 @@ __global__ void __launch_bounds__(128, QCB_CLOVER_MINB(R)) k_clover_qe(Geom g, L
     for (int64_t h = (int64_t)blockIdx.y * blockDim.x + threadIdx.x; h < g.Vh; h += (int64_t)gridDim.y * blockDim.x)
         site_clover_pair<R, NE, 3>(g, U, par, pair, (int)h, v);
     block_sum_store<3>(v, partials, blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// The measurement from the clover halves: per site, F of each plane = (half 0 + half 1) scaled as
+// clover_F scales its leaf sums, then q, e and the plaquette sum as site_clover_pair forms them.
+// One thread per site (site = parity * Vh + h), partials (q, e, p) per block.
+template <typename R>
+__global__ void __launch_bounds__(128) k_clover_halves(Geom g, HalfClovers<R> H, double* partials) {
+    double v[3] = {0.0, 0.0, 0.0};
+    const int64_t site = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (site < H.V) {
+        CloverF<R> F[6];
+        double pl = 0.0;
+#pragma unroll
+        for (int p = 0; p < 6; p++) {
+            R x[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++)
+                x[k] = H.p[(int64_t)((p * 2) * 9 + k) * H.V + site] + H.p[(int64_t)((p * 2 + 1) * 9 + k) * H.V + site];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                F[p].o[k] = scl((R)0.125, mkc<R>(x[2 * k], x[2 * k + 1]));
+                F[p].d[k] = (R)0.25 * x[6 + k];
+            }
+            pl += (double)H.p[(int64_t)(108 + p) * H.V + site];
+        }
+        // pairs 01-23 (+), 02-13 (-), 03-12 (+)
+        const double q = clover_re_tr(F[0], F[5]) - clover_re_tr(F[1], F[4]) + clover_re_tr(F[2], F[3]);
+        v[0] = q * (1.0 / (4.0 * kPi * kPi));
+        double e = 0.0;
+#pragma unroll
+        for (int p = 0; p < 6; p++) e += clover_sq_norm(F[p]);
+        v[1] = 0.5 * e;
+        v[2] = pl / 3.0;
+    }
+    block_sum_store<3>(v, partials, blockIdx.x);
 }
 
 // clover_site (observables_mpi.cpp:66-90) at one site, plane (mu, nu), as the 3x3 F (18 doubles), or

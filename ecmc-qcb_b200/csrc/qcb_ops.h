@@ -38,6 +38,10 @@ struct FmtOps {
                               cudaStream_t s);
     cudaError_t (*flow1)(const Geom& g, const void* win, void* wout, void* z, double eps, int stage, int reproject,
                          cudaStream_t s);
+    // stage 1 that also writes the clover halves of its input (hbuf: halves_bytes), and their sum
+    cudaError_t (*flow1_meas)(const Geom& g, const void* win, void* wout, void* z, double eps, int reproject,
+                              void* hbuf, cudaStream_t s);
+    cudaError_t (*clover_halves)(const Geom& g, const void* hbuf, double* partials, unsigned nb, cudaStream_t s);
     cudaError_t (*flow_force)(const Geom& g, const void* w, void* f, cudaStream_t s);
     cudaError_t (*flow_update)(const Geom& g, void* w, const void* f0, const void* f1, double a, double b, int use_f1,
                                int reproject, cudaStream_t s);

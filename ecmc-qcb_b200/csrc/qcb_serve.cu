@@ -36,6 +36,12 @@
 #include "qcb_internal.h"
 #include "qcb_ops.h"
 
+// Big requests take each measurement that an RK3 step follows from that step's stage 1 (clover
+// halves), as qcb_flow_measure does; 0 measures them with the clover pass every tick.
+#ifndef QCB_SERVE_FUSED_MEAS
+#define QCB_SERVE_FUSED_MEAS 1
+#endif
+
 using namespace qcb;
 
 namespace {
@@ -54,6 +60,7 @@ struct Request {
     int tick0 = 0;
     int flip = 0;
     cudaStream_t st = nullptr;  // the stream of all its work (big or small requests' stream)
+    double* meas_slot = nullptr;  // a big request's slot of this tick, filled by its next stage 1
 };
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -76,6 +83,8 @@ struct qcb_server_s {
     std::vector<Request*> small, big;  // the active set split by size (rebuild)
     double* big_partials = nullptr;
     size_t big_partials_cap = 0;
+    char* halves = nullptr;  // clover halves of a big request's measuring stage 1 (shared: one stream)
+    size_t halves_cap = 0;
     size_t bytes_in_use = 0, bytes_peak = 0;
     uint64_t submitted = 0, completed = 0;
     bool stop = false;
@@ -281,6 +290,28 @@ bool measure_big(qcb_server_s* s, Request* r, int flip_xor) {
     return cuda_ok(s, cudaGetLastError(), "measure finalize");
 }
 
+// Stage 1 of a big request's RK3 step that also measures its input, into r->meas_slot: the
+// measuring stage 1, the per-site sum of the clover halves and the finalize of qcb_flow_measure
+// (same kernels, same partial counts), so a big request's rows equal the plain measured flow's.
+bool flow_big_meas(qcb_server_s* s, Request* r, int flip_xor, int rep) {
+    const int f = (r->flip ^ flip_xor) & 1;
+    void* a = r->buf;
+    void* b = (char*)r->buf + r->off_out;
+    const unsigned nb = halves_blocks(r->g.Vh);
+    if (!grow(s, &s->halves, &s->halves_cap, halves_bytes(s->fmt, r->g.Vh))) return false;
+    if (!grow(s, &s->big_partials, &s->big_partials_cap, (size_t)nb * 3)) return false;
+    const FmtOps& o = fmt_ops(s->fmt);
+    if (!cuda_ok(s, o.flow1_meas(r->g, (f & 1) ? b : a, (f & 1) ? a : b, (char*)r->buf + r->off_z, r->eps, rep,
+                                 s->halves, s->stream),
+                 "flow launch"))
+        return false;
+    if (!cuda_ok(s, o.clover_halves(r->g, s->halves, s->big_partials, nb, s->stream), "clover launch")) return false;
+    k_finalize<<<1, 256, 0, s->stream>>>(s->big_partials, (int)nb, 3, 0u, r->meas_slot);
+    note_launches(3);
+    r->meas_slot = nullptr;
+    return cuda_ok(s, cudaGetLastError(), "measure finalize");
+}
+
 // One RK3 stage of a big request: stage s reads buffer A when (f + s - 1) is even (f = number
 // of RK3 steps since admission, mod 2) and writes the other buffer.
 bool flow_big(qcb_server_s* s, Request* r, int stage, int flip_xor, int rep) {
@@ -402,7 +433,14 @@ void scheduler(qcb_server_s* s) {
             s->tick_dev = s->tick + 1;
         }
         s->version_ticks++;
-        for (Request* r : s->big) ok = ok && measure_big(s, r, fx);
+        // a big request that flows on after this measurement takes it from its next stage 1;
+        // its last measurement (and every one without RK3 steps) uses the clover pass
+        for (Request* r : s->big) {
+            if (QCB_SERVE_FUSED_MEAS && s->n_rk > 0 && s->tick - r->tick0 != r->n_steps - 1)
+                r->meas_slot = (double*)((char*)r->buf + r->off_meas) + (size_t)(s->tick - r->tick0) * 3;
+            else
+                ok = ok && measure_big(s, r, fx);
+        }
         if (!ok) break;
         // requests that took their last measurement leave the mix
         std::vector<Request*> leaving, staying;
@@ -425,7 +463,9 @@ void scheduler(qcb_server_s* s) {
             for (int k = 0; k < s->n_rk && ok; k++) {
                 const int f = (f0 + k) & 1;
                 for (int stage = 1; stage <= 3 && ok; stage++)
-                    for (Request* r : s->big) ok = ok && flow_big(s, r, stage, f, rep);
+                    for (Request* r : s->big)
+                        ok = ok && (stage == 1 && r->meas_slot ? flow_big_meas(s, r, f, rep)
+                                                               : flow_big(s, r, stage, f, rep));
             }
             s->nflow += (uint64_t)s->n_rk;
         }
@@ -517,6 +557,7 @@ int qcb_serve_destroy(qcb_server s) {
     if (s->d_tile_lat) cudaFree(s->d_tile_lat);
     if (s->partials) cudaFree(s->partials);
     if (s->big_partials) cudaFree(s->big_partials);
+    if (s->halves) cudaFree(s->halves);
     if (s->staging) cudaFree(s->staging);
     if (s->pool) cudaMemPoolDestroy(s->pool);
     if (s->stream) cudaStreamDestroy(s->stream);

@@ -337,3 +337,32 @@ def test_flow_graphs_match_plain_launches(gpu, orc, prec, store):
         tb, pb = b.measure(f, 6, n_rk, plaquette=True)
         assert np.array_equal(ta, tb) and np.array_equal(pa, pb), n_rk
         assert np.array_equal(a.field.download(), b.field.download()), n_rk
+
+
+@pytest.mark.parametrize("prec,store", [(64, 0), (64, 1), (32, 0), (32, 1)])
+def test_measured_flow_from_stage1_matches_clover_pass(gpu, orc, prec, store):
+    """qcb_flow_measure takes each measurement (Q, E, plaquette) of a configuration that an RK3 step
+    follows from that step's stage 1 (clover halves of the force's staples) instead of a clover
+    pass.  Every row equals the clover pass on the same configuration: to 1e-12 in FP64 (Q to
+    1e-12 * sum |q|), to FP32 rounding in FP32; the flowed links are those of plain RK3 steps."""
+    L = (8, 6, 4, 10)
+    U = orc.hot_start(L, 31)
+    orc.hb_sweep(U, L, 6.0, 2, 32, 0)
+    f = gpu.GaugeField(L, 64, 0)
+    f.upload(U)
+    tol = TOL if prec == 64 else 2e-6
+    qscale = max(1.0, float(np.abs(orc.clover_qe_density(U, L)[0]).sum()))
+    for n_rk in (1, 2):
+        a = gpu.GradientFlow(f, 0.02, prec=prec, store=store)
+        t, p = a.measure(f, 5, n_rk, plaquette=True)
+        b = gpu.GradientFlow(f, 0.02, prec=prec, store=store)
+        for s in range(5):
+            Q, E = b.field.clover_qe()
+            assert abs(t[s, 1] - Q) < tol * qscale, (n_rk, s)
+            assert abs(t[s, 2] - E) < tol * abs(E), (n_rk, s)
+            assert abs(p[s] - b.field.plaquette()) < tol, (n_rk, s)
+            if s < 4:
+                b.rk3_step(n_rk)
+        assert np.array_equal(a.field.download(), b.field.download()), n_rk
+        a.close()
+        b.close()

@@ -31,6 +31,9 @@ def run(server, reqs, timeout=300.0):
 
 @pytest.mark.parametrize("prec,store", [(32, 0), (32, 1), (64, 0)])
 def test_alone_equals_plain_flow(gpu, prec, store):
+    """The server measures a small request with the batched clover pass; qcb_flow_measure takes each
+    measurement that a step follows from that step's stage 1 (clover halves).  The two agree to
+    1e-10 in Q and 1e-12 in E in FP64, to FP32 rounding in FP32."""
     f, U = config(gpu, (8, 8, 8, 8), 11)
     s = gpu.Server(1 << 30, prec=prec, store=store)
     res = run(s, [(7, f.L, U, 6)])
@@ -39,8 +42,9 @@ def test_alone_equals_plain_flow(gpu, prec, store):
     fl = gpu.GradientFlow(f, EPS, prec=prec, store=store)
     ref = fl.measure(f, 6, 1)
     assert np.array_equal(tqe[:, 0], ref[:, 0])
-    assert np.max(np.abs(tqe[:, 1] - ref[:, 1])) < 1e-10
-    assert np.max(np.abs(tqe[:, 2] - ref[:, 2]) / ref[:, 2]) < 1e-12
+    dq, de = (1e-10, 1e-12) if prec == 64 else (2e-6, 2e-6)
+    assert np.max(np.abs(tqe[:, 1] - ref[:, 1])) < dq
+    assert np.max(np.abs(tqe[:, 2] - ref[:, 2]) / ref[:, 2]) < de
     t_sub, t_adm, t_done = res[7][2]
     assert t_sub <= t_adm <= t_done
 
