@@ -694,12 +694,17 @@ def run_ours(args, rank: int, world: int, local: int):
         f.close()
         return
 
-    if args.only == "flow":
+    if args.only in ("flow", "mflow"):
         for i in range(args.warmup):
             f.hb_sweep(BETA, N_HITS, SEED_HB, i)
         fma_peak = {64: qcb.fma_rate(64) / 1e12, 32: qcb.fma_rate(32) / 1e12}
         for prec, store in ((64, 0), (32, 0), (32, 1)):
-            flow_block(qcb, f, prec, store, args.steps, hbm_peak, fma_peak, local, measured=False)
+            if args.only == "mflow":  # the measured flow alone (ncu captures of its kernels)
+                fl = qcb.GradientFlow(f, 0.02, prec=prec, store=store)
+                fl.measure(f, args.steps + 1, 1, plaquette=True)
+                fl.close()
+            else:
+                flow_block(qcb, f, prec, store, args.steps, hbm_peak, fma_peak, local, measured=False)
         f.close()
         return
 
@@ -858,7 +863,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="length of the CPU-baseline sample (0 skips it)")
-    ap.add_argument("--only", default="all", choices=["all", "hb", "flow", "obs", "batch", "serve"],
+    ap.add_argument("--only", default="all", choices=["all", "hb", "flow", "mflow", "obs", "batch", "serve"],
                     help="run one part (used for ncu captures of a single kernel family)")
     ap.add_argument("--parts", default="all", choices=["all", "core"],
                     help="core: skip the batch and serving sections")
