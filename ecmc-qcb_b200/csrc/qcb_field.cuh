@@ -28,7 +28,8 @@ namespace qcb {
 // Checked build (libqcb_checked.so): every (mu, parity, h) that a link or algebra access is
 // formed from is validated on the device before the address is.  A bad one is counted in this
 // translation unit's record, the first is kept as kind << 62 | (mu & 63) << 56 | (par & 255) << 48
-// | (h mod 2^48) (kind 0 = link, 1 = su(3) algebra), and the access is redirected to link
+// | (h mod 2^48) (kind 0 = link, 1 = su(3) algebra, 2 = clover halves: mu = the real mod 64, parity = 1 past the
+// sites), and the access is redirected to link
 // (0, 0, 0), inside the allocation, so the kernel runs on instead of faulting.  The host reads
 // and clears every translation unit's record through qcb_debug_oob.
 static __device__ unsigned long long g_oob_count;

@@ -236,13 +236,27 @@ template <typename R>
 struct HalfClovers {
     R* p;
     int64_t V;
+    // offset of real k of a site; the checked build validates (k, site) as it does link indices
+    // (kind 2) and redirects a bad one to real 0 of site 0
+    __device__ __forceinline__ int64_t at(int k, int64_t site) const {
+#if defined(QCB_CHECKED) && defined(__CUDA_ARCH__)
+        if (!((unsigned)k < (unsigned)(6 * 2 * 9 + 6) && site >= 0 && site < V)) {
+            note_oob(2, k, site >= V ? 1 : 0, site);
+            k = 0;
+            site = 0;
+        }
+#endif
+        return (int64_t)k * V + site;
+    }
     __device__ __forceinline__ void put_half(int plane, int half, int64_t site, const R v[9], R sign) const {
 #pragma unroll
-        for (int k = 0; k < 9; k++) p[(int64_t)((plane * 2 + half) * 9 + k) * V + site] = sign * v[k];
+        for (int k = 0; k < 9; k++) p[at((plane * 2 + half) * 9 + k, site)] = sign * v[k];
     }
-    __device__ __forceinline__ void put_plaq(int plane, int64_t site, R tr) const {
-        p[(int64_t)(108 + plane) * V + site] = tr;
+    __device__ __forceinline__ void put_plaq(int plane, int64_t site, R tr) const { p[at(108 + plane, site)] = tr; }
+    __device__ __forceinline__ R half(int plane, int half, int k, int64_t site) const {
+        return p[at((plane * 2 + half) * 9 + k, site)];
     }
+    __device__ __forceinline__ R plaq(int plane, int64_t site) const { return p[at(108 + plane, site)]; }
 };
 
 // acc(A B) for full 3x3 A, B: the six off-diagonal entries of A B and the imaginary parts of its
@@ -1317,14 +1331,13 @@ __global__ void __launch_bounds__(128) k_clover_halves(Geom g, HalfClovers<R> H,
         for (int p = 0; p < 6; p++) {
             R x[9];
 #pragma unroll
-            for (int k = 0; k < 9; k++)
-                x[k] = H.p[(int64_t)((p * 2) * 9 + k) * H.V + site] + H.p[(int64_t)((p * 2 + 1) * 9 + k) * H.V + site];
+            for (int k = 0; k < 9; k++) x[k] = H.half(p, 0, k, site) + H.half(p, 1, k, site);
 #pragma unroll
             for (int k = 0; k < 3; k++) {
                 F[p].o[k] = scl((R)0.125, mkc<R>(x[2 * k], x[2 * k + 1]));
                 F[p].d[k] = (R)0.25 * x[6 + k];
             }
-            pl += (double)H.p[(int64_t)(108 + p) * H.V + site];
+            pl += (double)H.plaq(p, site);
         }
         // pairs 01-23 (+), 02-13 (-), 03-12 (+)
         const double q = clover_re_tr(F[0], F[5]) - clover_re_tr(F[1], F[4]) + clover_re_tr(F[2], F[3]);
