@@ -121,9 +121,12 @@ struct qcb_server_s {
     int* d_tick = nullptr;  // the tick the device's finalize kernels write (advanced on the device)
     int tick_dev = 0;       // the value d_tick holds once the enqueued work has run
     int tick_copy = 0;      // host source of a d_tick reset
-    // counters
-    int tick = 0;       // measurements taken by the scheduler (slot index base)
-    uint64_t nflow = 0; // RK3 steps executed (buffer parity)
+    // counters of the two request sets, which tick at their own pace: measurements taken (slot
+    // index base) and RK3 steps executed (buffer parity) of the small set, then of the big set
+    int tick = 0;
+    uint64_t nflow = 0;
+    int tick_b = 0;
+    uint64_t nflow_b = 0;
     uint64_t ticks = 0;
     int active_peak = 0;
     double busy = 0.0;
@@ -245,8 +248,8 @@ bool admit(qcb_server_s* s, Request* r) {
     if (!cuda_ok(s, cudaEventRecord(s->ev_layout, r->st), "layout event")) return false;
     s->layout_pending = true;
     std::vector<double>().swap(r->input);
-    r->tick0 = s->tick;
-    r->flip = (int)(s->nflow & 1);  // current links in buffer A
+    r->tick0 = is_big(r) ? s->tick_b : s->tick;
+    r->flip = (int)((is_big(r) ? s->nflow_b : s->nflow) & 1);  // current links in buffer A
     return true;
 }
 
@@ -284,7 +287,7 @@ bool measure_big(qcb_server_s* s, Request* r, int flip_xor) {
     if (!cuda_ok(s, fmt_ops(s->fmt).clover(r->g, current_links(r, flip_xor), s->big_partials, nbx, s->stream),
                  "clover launch"))
         return false;
-    double* slot = (double*)((char*)r->buf + r->off_meas) + (size_t)(s->tick - r->tick0) * 3;
+    double* slot = (double*)((char*)r->buf + r->off_meas) + (size_t)(s->tick_b - r->tick0) * 3;
     k_finalize<<<1, 256, 0, s->stream>>>(s->big_partials, (int)(nbx * 6), 3, 0u, slot);
     note_launches(2);
     return cuda_ok(s, cudaGetLastError(), "measure finalize");
@@ -388,6 +391,106 @@ void drop_tick_graphs(qcb_server_s* s) {
         }
 }
 
+// Small-request ticks a scheduler round runs beside one big-request tick, so that the two streams
+// get similar work and a small request does not wait for the big ones' steps: the big set's sites
+// over the small set's (the shared tile kernels cost about a third more a site), 1 to 8.
+constexpr int kMaxSmallTicks = 8;
+int small_ticks(const qcb_server_s* s) {
+    if (s->big.empty() || s->small.empty()) return 1;
+    double vb = 0.0, vs = 0.0;
+    for (const Request* r : s->big) vb += (double)r->g.V;
+    for (const Request* r : s->small) vs += (double)r->g.V;
+    return std::min(kMaxSmallTicks, std::max(1, (int)(vb / (1.3 * vs) + 0.5)));
+}
+
+WorkList small_worklist(const qcb_server_s* s) {
+    WorkList w;
+    w.lats = s->d_desc;
+    w.tile_lat = s->d_tile_lat;
+    w.nb_total = s->nb_total;
+    w.nlat = (int)s->small.size();
+    return w;
+}
+
+// Requests that took their last measurement leave: results read back, memory returned, published.
+bool retire(qcb_server_s* s, const std::vector<Request*>& leaving) {
+    if (leaving.empty()) return true;
+    for (Request* r : leaving)
+        if (!finish(s, r)) return false;
+    std::vector<Request*> staying;
+    for (Request* r : s->active)
+        if (std::find(leaving.begin(), leaving.end(), r) == leaving.end()) staying.push_back(r);
+    s->active.swap(staying);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (Request* r : leaving) {
+            s->bytes_in_use -= r->bytes;
+            s->done.push_back(r);
+            s->completed++;
+        }
+        s->cv_done.notify_all();
+    }
+    return rebuild(s);
+}
+
+// One tick of the big requests (single-lattice kernels on the big stream): measure each at its
+// current step, retire those done, advance the others by n_rk RK3 steps.
+bool big_tick(qcb_server_s* s, int rep) {
+    const int fx = (int)(s->nflow_b & 1);
+    bool ok = true;
+    // a big request that flows on after this measurement takes it from its next stage 1;
+    // its last measurement uses the clover pass
+    for (Request* r : s->big) {
+        if (QCB_SERVE_FUSED_MEAS && s->tick_b - r->tick0 != r->n_steps - 1)
+            r->meas_slot = (double*)((char*)r->buf + r->off_meas) + (size_t)(s->tick_b - r->tick0) * 3;
+        else
+            ok = ok && measure_big(s, r, fx);
+    }
+    if (!ok) return false;
+    std::vector<Request*> leaving;
+    for (Request* r : s->big)
+        if (s->tick_b - r->tick0 == r->n_steps - 1) leaving.push_back(r);
+    s->tick_b++;
+    if (!retire(s, leaving)) return false;
+    const int f0 = (int)(s->nflow_b & 1);
+    for (int k = 0; k < s->n_rk && ok; k++) {
+        const int f = (f0 + k) & 1;
+        for (int stage = 1; stage <= 3 && ok; stage++)
+            for (Request* r : s->big)
+                ok = ok && (stage == 1 && r->meas_slot ? flow_big_meas(s, r, f, rep) : flow_big(s, r, stage, f, rep));
+    }
+    s->nflow_b += (uint64_t)s->n_rk;
+    return ok;
+}
+
+// One tick of the small requests (shared tile launches on the small stream, replayed from graphs
+// while the set is unchanged): measure, retire those done, advance the others.
+bool small_tick(qcb_server_s* s, int rep) {
+    WorkList w = small_worklist(s);
+    const int fx = (int)(s->nflow & 1);
+    if (s->tick_dev != s->tick) {  // a reset of the set left the device counter behind
+        s->tick_copy = s->tick;
+        if (!cuda_ok(s, cudaMemcpyAsync(s->d_tick, &s->tick_copy, sizeof(int), cudaMemcpyHostToDevice,
+                                        s->stream_small), "tick counter"))
+            return false;
+    }
+    if (!small_run(s, s->gmeas, fx, [&] { return small_measure(s, w, fx); })) return false;
+    s->tick_dev = s->tick + 1;
+    s->version_ticks++;
+    std::vector<Request*> leaving;
+    for (Request* r : s->small)
+        if (s->tick - r->tick0 == r->n_steps - 1) leaving.push_back(r);
+    s->tick++;
+    if (!retire(s, leaving)) return false;
+    if (!s->small.empty()) {
+        w = small_worklist(s);
+        const int f0 = (int)(s->nflow & 1);
+        if (!small_run(s, s->gflow, f0, [&] { return small_flow(s, w, f0, rep); })) return false;
+    }
+    s->nflow += (uint64_t)s->n_rk;
+    return true;
+}
+
 void scheduler(qcb_server_s* s) {
     cudaSetDevice(s->device);
     const int rep = needs_reproject(s->prec, s->store);
@@ -415,72 +518,17 @@ void scheduler(qcb_server_s* s) {
         if (ok && !fresh.empty()) ok = rebuild(s);
         if (!ok) break;
         if (s->active.empty()) continue;
-        // measure every resident request at its current step
-        WorkList w;
-        w.lats = s->d_desc;
-        w.tile_lat = s->d_tile_lat;
-        w.nb_total = s->nb_total;
-        w.nlat = (int)s->small.size();
-        const int fx = (int)(s->nflow & 1);
-        if (!s->small.empty()) {
-            if (s->tick_dev != s->tick) {  // ticks without small requests left the device counter behind
-                s->tick_copy = s->tick;
-                if (!cuda_ok(s, cudaMemcpyAsync(s->d_tick, &s->tick_copy, sizeof(int), cudaMemcpyHostToDevice,
-                                                s->stream_small), "tick counter"))
-                    break;
-            }
-            if (!small_run(s, s->gmeas, fx, [&] { return small_measure(s, w, fx); })) break;
-            s->tick_dev = s->tick + 1;
-        }
-        s->version_ticks++;
-        // a big request that flows on after this measurement takes it from its next stage 1;
-        // its last measurement (and every one without RK3 steps) uses the clover pass
-        for (Request* r : s->big) {
-            if (QCB_SERVE_FUSED_MEAS && s->n_rk > 0 && s->tick - r->tick0 != r->n_steps - 1)
-                r->meas_slot = (double*)((char*)r->buf + r->off_meas) + (size_t)(s->tick - r->tick0) * 3;
-            else
-                ok = ok && measure_big(s, r, fx);
-        }
-        if (!ok) break;
-        // requests that took their last measurement leave the mix
-        std::vector<Request*> leaving, staying;
-        for (Request* r : s->active) (s->tick - r->tick0 == r->n_steps - 1 ? leaving : staying).push_back(r);
-        s->tick++;
-        for (Request* r : leaving) ok = ok && finish(s, r);
-        if (!ok) break;
-        if (!leaving.empty()) {
-            s->active.swap(staying);
-            if (!rebuild(s)) break;
-            w.lats = s->d_desc;
-            w.tile_lat = s->d_tile_lat;
-            w.nb_total = s->nb_total;
-            w.nlat = (int)s->small.size();
-        }
-        if (!s->active.empty()) {
-            const int f0 = (int)(s->nflow & 1);
-            if (!s->small.empty())
-                ok = small_run(s, s->gflow, f0, [&] { return small_flow(s, w, f0, rep); });
-            for (int k = 0; k < s->n_rk && ok; k++) {
-                const int f = (f0 + k) & 1;
-                for (int stage = 1; stage <= 3 && ok; stage++)
-                    for (Request* r : s->big)
-                        ok = ok && (stage == 1 && r->meas_slot ? flow_big_meas(s, r, f, rep)
-                                                               : flow_big(s, r, stage, f, rep));
-            }
-            s->nflow += (uint64_t)s->n_rk;
-        }
+        const int n_active = (int)s->active.size();
+        // one round: a tick of the big requests and m ticks of the small ones
+        const int m = small_ticks(s);
+        if (!s->big.empty()) ok = big_tick(s, rep);
+        for (int j = 0; ok && j < m && !s->small.empty(); j++) ok = small_tick(s, rep);
         if (!ok) break;
         {
             std::lock_guard<std::mutex> lk(s->mu);
             s->ticks++;
-            s->active_peak = std::max(s->active_peak, (int)s->active.size() + (int)leaving.size());
+            s->active_peak = std::max(s->active_peak, n_active);
             s->busy += s->now() - tb;
-            for (Request* r : leaving) {
-                s->bytes_in_use -= r->bytes;
-                s->done.push_back(r);
-                s->completed++;
-            }
-            if (!leaving.empty()) s->cv_done.notify_all();
         }
     }
     cudaStreamSynchronize(s->stream);

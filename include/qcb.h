@@ -293,7 +293,8 @@ int qcb_serve_submit(qcb_server s, uint64_t id, const int L[4], const double* li
 int qcb_serve_poll(qcb_server s, uint64_t* id, double* tQE, int max_steps, int* n_steps, double* times);
 /* Waits at most timeout_s seconds for every submitted request to complete (QCB_ETIMEOUT otherwise). */
 int qcb_serve_wait(qcb_server s, double timeout_s);
-/* out[8]: submitted, completed, ticks, peak resident, peak bytes, bytes in use, busy s, queued. */
+/* out[8]: submitted, completed, scheduler rounds (a tick of the big requests and 1-8 ticks of the
+ * small ones), peak resident, peak bytes, bytes in use, busy s, queued. */
 int qcb_serve_stats(qcb_server s, double* out);
 
 /* ------------------------------------------------------------------ allocation-free entry */
