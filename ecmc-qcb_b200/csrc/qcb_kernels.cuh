@@ -441,8 +441,10 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
 #ifndef QCB_FLOW_THREADS
 #define QCB_FLOW_THREADS 128
 #endif
+// shared (tile) flow stage of the server's small requests: FP32 at 5 blocks/SM (102 registers, no
+// spills; 24 resident 16^4 requests x 300 steps 0.83-0.90 s against 0.91-0.95 s at 6)
 #ifndef QCB_FLOW_MINB
-#define QCB_FLOW_MINB(R) (sizeof(R) == 8 ? 3 : 6)
+#define QCB_FLOW_MINB(R) (sizeof(R) == 8 ? 3 : 5)
 #endif
 // Clover kernels: 2 resident blocks per SM for FP64, 4 for FP32 (32^4 clover pass 1.02 ms FP64 and
 // 0.49 ms FP32 against 1.24 ms and 0.69 ms at 3 and 6).
@@ -454,7 +456,7 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
 #define QCB_FLOW1_THREADS QCB_FLOW_THREADS
 #endif
 #ifndef QCB_FLOW1_MINB
-#define QCB_FLOW1_MINB(R) QCB_FLOW_MINB(R)
+#define QCB_FLOW1_MINB(R) (sizeof(R) == 8 ? 3 : 6)
 #endif
 // stage 1 with the clover halves: the forward staple is held until the backward one is formed
 #ifndef QCB_FLOW_MEAS_MINB
