@@ -213,3 +213,56 @@ def test_projection_su3(orc):
     P = orc.projection_su3(M)
     assert np.max(np.abs(P @ P.conj().T - np.eye(3))) < 1e-14
     assert abs(np.linalg.det(P) - 1) < 1e-14
+
+
+def test_clover_halves_from_staple_differences(orc):
+    """The measured flow's clover (k_flow_stage1_meas + k_clover_halves) rests on this identity: with
+    D(y) the forward minus the backward staple of link (y, mu) in plane nu (the oracle's staple
+    terms), acc(sum of the four leaves of x) = acc(U_mu(x) D(x)) + acc(D(x - mu) U_mu(x - mu)), where
+    acc(M) = (M_ij - conj(M_ji) for i < j, Im M_ii).  From the nu links the same plane comes with the
+    orientation reversed and the sign of acc flipped."""
+    L = (4, 6, 2, 4)
+    U = orc.hot_start(L, 17)
+    V = int(np.prod(L))
+
+    def co(i):
+        c = []
+        for d in range(4):
+            c.append(i % L[d])
+            i //= L[d]
+        return c
+
+    def mv(i, d, s):
+        c = co(i)
+        c[d] = (c[d] + s) % L[d]
+        return c[0] + L[0] * (c[1] + L[1] * (c[2] + L[2] * c[3]))
+
+    def dag(m):
+        return m.conj().T
+
+    def acc(m):
+        return np.array([m[0, 1] - np.conj(m[1, 0]), m[0, 2] - np.conj(m[2, 0]), m[1, 2] - np.conj(m[2, 1]),
+                         m[0, 0].imag, m[1, 1].imag, m[2, 2].imag])
+
+    def leaves(x, mu, nu):  # observables_mpi.cpp:66-90, the four leaves in the reference's order
+        xm, xn, xmm, xmn = mv(x, mu, 1), mv(x, nu, 1), mv(x, mu, -1), mv(x, nu, -1)
+        return (U[x, mu] @ U[xm, nu] @ dag(U[xn, mu]) @ dag(U[x, nu])
+                + U[x, nu] @ dag(U[mv(xmm, nu, 1), mu]) @ dag(U[xmm, nu]) @ U[xmm, mu]
+                + dag(U[xmm, mu]) @ dag(U[mv(xmm, nu, -1), nu]) @ U[mv(xmm, nu, -1), mu] @ U[xmn, nu]
+                + dag(U[xmn, nu]) @ U[xmn, mu] @ U[mv(xm, nu, -1), nu] @ dag(U[x, mu]))
+
+    def D(y, mu, nu):  # compute_staple's two terms of plane nu (GaugeField.cpp:74-97)
+        sf = U[mv(y, mu, 1), nu] @ dag(U[mv(y, nu, 1), mu]) @ dag(U[y, nu])
+        sb = dag(U[mv(mv(y, mu, 1), nu, -1), nu]) @ dag(U[mv(y, nu, -1), mu]) @ U[mv(y, nu, -1), nu]
+        return sf - sb
+
+    err = 0.0
+    for x in range(V):
+        for mu in range(4):
+            for nu in range(mu + 1, 4):
+                a = acc(leaves(x, mu, nu))
+                y, z = mv(x, mu, -1), mv(x, nu, -1)
+                b = acc(U[x, mu] @ D(x, mu, nu)) + acc(D(y, mu, nu) @ U[y, mu])
+                c = -(acc(U[x, nu] @ D(x, nu, mu)) + acc(D(z, nu, mu) @ U[z, nu]))
+                err = max(err, np.abs(a - b).max(), np.abs(a - c).max())
+    assert err < 1e-13
