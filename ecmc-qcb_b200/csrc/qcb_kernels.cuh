@@ -216,8 +216,8 @@ __device__ __forceinline__ M3<R> staple_rt_rows(const Geom& g, const LinkField<R
 // linear and odd under the adjoint.  With D(y) = S_f(y) - S_b(y), the forward minus the backward
 // staple of link (y, mu) in plane nu (the two terms compute_staple sums for that plane),
 //   leaves 1 + 4 of x:  acc(U_mu(x) D(x)),      leaves 2 + 3 of x:  acc(D(x - mu) U_mu(x - mu)),
-// since leaf 1 = U_mu(x) S_f(x), leaf 4 = (U_mu(x) S_b(x))^dag, leaf 2 = (S_f(x-mu) U_mu(x-mu))^dag
-// and leaf 3 = S_b(x-mu) U_mu(x-mu) up to the adjoint's sign.  Stage 1 of an RK3 step forms S_f and
+// since leaf 1 = U_mu(x) S_f(x), leaf 4 = (U_mu(x) S_b(x))^dag, leaf 2 = S_f(x-mu) U_mu(x-mu) and
+// leaf 3 = (S_b(x-mu) U_mu(x-mu))^dag, and acc(X^dag) = -acc(X).  Stage 1 of an RK3 step forms S_f and
 // S_b of every link for its force, so with two more products a plane (U D and D U) it yields the
 // clover of its input configuration: the link (y, mu) writes the half for leaves 1 + 4 of y and the
 // half for leaves 2 + 3 of y + mu, and k_clover_halves adds the two halves of each site.  From the
