@@ -243,6 +243,22 @@ int flow_step_meas(qcb_flow_s* fl, double* dst) {
     return QCB_OK;
 }
 
+// The measurement of the flowed field alone through the measuring stage 1 (its stage-1 output, in
+// the spare buffer, is left unused): the last measurement of a run, so that every row of a measured
+// flow comes from the same arithmetic.
+int meas_halves_only(qcb_flow_s* fl, double* dst) {
+    qcb_field_s* f = fl->fld;
+    RET(ensure_alt(f));
+    const int rep = needs_reproject(f->prec, f->store);
+    RET(launch(f, QCB_K_CLOVER, [&] {
+        return fmt_ops(f->fmt).flow1_meas(f->g, f->links, f->alt, fl->z, fl->eps, rep, fl->halves, f->stream);
+    }));
+    const unsigned nb = halves_blocks(f->g.Vh);
+    RET(launch(f, QCB_K_CLOVER,
+               [&] { return fmt_ops(f->fmt).clover_halves(f->g, fl->halves, f->partials, nb, f->stream); }));
+    return finalize(f, (int)nb, 3, 0u, dst);
+}
+
 // ------------------------------------------------------------------ flow step graphs
 // Without per-launch timing, the flow's repeated launch sequences are captured once as CUDA graphs
 // and replayed: two RK3 steps (six stage launches; the ping-pong buffers are back in place after
@@ -328,15 +344,17 @@ int flow_graph_run(qcb_flow_s* fl, int kind, int n_rk) {
 }
 
 // One measurement of the flowed field -- (q, e and the plaquette sum) into the fixed slot, copied to
-// the next row of the measurement buffer -- followed by n_rk RK3 steps.  With a step to follow
-// (and the halves buffer in place) the measurement comes from that step's stage 1; the last
-// measurement of a run uses the clover pass.
+// the next row of the measurement buffer -- followed by n_rk RK3 steps.  With the halves buffer in
+// place (measured flows with RK3 steps) the measurement comes from the measuring stage 1: that of
+// the following step, or for the last measurement one whose output is left unused.
 int meas_block(qcb_flow_s* fl, int n_rk) {
     qcb_field_s* f = fl->fld;
     double* slot = f->d_res + kMeasSlot;
     const bool fused = n_rk > 0 && fl->halves;
     if (fused)
         RET(flow_step_meas(fl, slot));
+    else if (fl->halves)
+        RET(meas_halves_only(fl, slot));
     else
         RET(enq_clover(f, slot));
     RET(launch(f, QCB_K_OTHER, [&] {
@@ -936,7 +954,7 @@ int qcb_flow_measure(qcb_flow fl, qcb_field src, int n_steps, int n_rk, double* 
     RET(ensure_partials(f, std::max((size_t)clover_blocks(f->g.Vh) * 18, (size_t)halves_blocks(f->g.Vh) * 3)));
 #if QCB_FLOW_FUSED_MEAS
     // the clover halves of the measuring stage 1, allocated before any graph capture
-    if (n_rk > 0 && n_steps > 1 && !fl->halves) CK(cudaMalloc(&fl->halves, halves_bytes(f->fmt, f->g.Vh)));
+    if (n_rk > 0 && !fl->halves) CK(cudaMalloc(&fl->halves, halves_bytes(f->fmt, f->g.Vh)));
 #endif
     CK(cudaMemsetAsync(fl->d_count, 0, sizeof(int), f->stream));
     const bool graphs = graphs_ok(f) && n_rk > 0;

@@ -179,6 +179,20 @@ struct FmtImpl {
         return cudaGetLastError();
     }
 
+    static cudaError_t flow_tiles1_meas(const WorkList& w, int flip_xor, int rep, cudaStream_t s) {
+        static int cache = 0;
+        auto k = k_flow_tiles1_meas<R, NE>;
+        const int ntiles = 8 * w.nb_total;
+        const int grid = std::min(ntiles, resident_blocks(k, QCB_FLOW_THREADS, &cache));
+        k<<<grid, QCB_FLOW_THREADS, 0, s>>>(w.lats, w.tile_lat, w.one, ntiles, flip_xor, rep);
+        return cudaGetLastError();
+    }
+    static cudaError_t halves_tiles(const WorkList& w, double* partials, cudaStream_t s) {
+        const int ntiles = 2 * w.nb_total;
+        k_halves_tiles<R><<<ntiles, TILE, 0, s>>>(w.lats, w.tile_lat, w.one, ntiles, partials);
+        return cudaGetLastError();
+    }
+
     static cudaError_t plaquette(const Geom& g, const void* links, double* partials, unsigned nbx, cudaStream_t s) {
         k_plaquette<R, NE><<<dim3(2, nbx), 256, 0, s>>>(g, view(links, g.Vh), partials);
         return cudaGetLastError();
@@ -236,6 +250,8 @@ struct FmtImpl {
         o.probe_link = &probe_link;
         o.flow1 = &flow1;
         o.flow1_meas = &flow1_meas;
+        o.flow_tiles1_meas = &flow_tiles1_meas;
+        o.halves_tiles = &halves_tiles;
         o.clover_halves = &clover_halves;
         o.flow_force = &flow_force;
         o.flow_update = &flow_update;

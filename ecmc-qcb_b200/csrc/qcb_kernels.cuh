@@ -1323,10 +1323,8 @@ __global__ void __launch_bounds__(128, QCB_CLOVER_MINB(R)) k_clover_qe(Geom g, L
 // clover_F scales its leaf sums, then q, e and the plaquette sum as site_clover_pair forms them.
 // One thread per site (site = parity * Vh + h), partials (q, e, p) per block.
 template <typename R>
-__global__ void __launch_bounds__(128) k_clover_halves(Geom g, HalfClovers<R> H, double* partials) {
-    double v[3] = {0.0, 0.0, 0.0};
-    const int64_t site = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (site < H.V) {
+__device__ __forceinline__ void site_halves_qe(const HalfClovers<R>& H, int64_t site, double v[3]) {
+    {
         CloverF<R> F[6];
         double pl = 0.0;
 #pragma unroll
@@ -1350,6 +1348,12 @@ __global__ void __launch_bounds__(128) k_clover_halves(Geom g, HalfClovers<R> H,
         v[1] = 0.5 * e;
         v[2] = pl / 3.0;
     }
+}
+template <typename R>
+__global__ void __launch_bounds__(128) k_clover_halves(Geom g, HalfClovers<R> H, double* partials) {
+    double v[3] = {0.0, 0.0, 0.0};
+    const int64_t site = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (site < H.V) site_halves_qe(H, site, v);
     block_sum_store<3>(v, partials, blockIdx.x);
 }
 

@@ -29,6 +29,10 @@ struct FmtOps {
     cudaError_t (*flow)(const WorkList& w, int stage, int flip_xor, int reproject, cudaStream_t s);
     cudaError_t (*plaq_tiles)(const WorkList& w, int flip_xor, double* partials, cudaStream_t s);
     cudaError_t (*clover_tiles)(const WorkList& w, int flip_xor, double* partials, cudaStream_t s);
+    // the tiled measuring stage 1 (clover halves into each LatDesc's `halves`) and their sums, two
+    // (q, e) partials a lattice block of sites
+    cudaError_t (*flow_tiles1_meas)(const WorkList& w, int flip_xor, int reproject, cudaStream_t s);
+    cudaError_t (*halves_tiles)(const WorkList& w, double* partials, cudaStream_t s);
     // ---- single-lattice kernels
     cudaError_t (*hb1)(const Geom& g, void* links, int par, int mu, double c_alpha, int n_hits, uint64_t seed,
                        uint32_t sweep, int reproject, int* err, cudaStream_t s);

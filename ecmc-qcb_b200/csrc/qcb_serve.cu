@@ -36,8 +36,9 @@
 #include "qcb_internal.h"
 #include "qcb_ops.h"
 
-// Big requests take each measurement that an RK3 step follows from that step's stage 1 (clover
-// halves), as qcb_flow_measure does; 0 measures them with the clover pass every tick.
+// Requests take every measurement from a measuring stage 1 (clover halves), as qcb_flow_measure
+// does: that of the RK3 step that follows it, or for the last one a stage 1 whose output is left
+// unused; 0 measures with clover passes.
 #ifndef QCB_SERVE_FUSED_MEAS
 #define QCB_SERVE_FUSED_MEAS 1
 #endif
@@ -57,6 +58,7 @@ struct Request {
     void* buf = nullptr;  // W, W', Z, measurements in one allocation
     size_t bytes = 0;
     size_t off_out = 0, off_z = 0, off_meas = 0;
+    size_t off_halves = 0;  // small requests: clover halves of the tiled measuring stage 1 (0: none)
     int tick0 = 0;
     int flip = 0;
     cudaStream_t st = nullptr;  // the stream of all its work (big or small requests' stream)
@@ -136,15 +138,15 @@ struct qcb_server_s {
 
 namespace {
 
-// Per-request deterministic sums of clover partials, stored in the request's slot of this tick:
-// meas[(tick - tick0) * 3 + k] = (Q, sum e) (k = 0, 1; slot k = 2 is the plaquette sum, which
-// only the single-lattice path measures).
+// Per-request deterministic sums of (q, e) partials, m tiles a lattice block of sites, stored in the
+// request's slot of this tick: meas[(tick - tick0) * 3 + k] = (Q, sum e) (k = 0, 1; slot k = 2 is
+// the plaquette sum, which only the single-lattice path measures).
 __global__ void k_meas_finalize(const LatDesc* __restrict__ lats, const double* __restrict__ partials,
-                                const int* __restrict__ d_tick) {
+                                const int* __restrict__ d_tick, int m) {
     __shared__ double sm[256];
     const int tick = *d_tick;
     const LatDesc* d = lats + blockIdx.x;
-    const int t0 = 6 * d->nb_begin, nt = 6 * d->nb;
+    const int t0 = m * d->nb_begin, nt = m * d->nb;
     for (int k = 0; k < 2; k++) {
         double acc = 0.0;
         for (int i = threadIdx.x; i < nt; i += 256) acc += partials[(size_t)(t0 + i) * 2 + k];
@@ -209,6 +211,7 @@ bool rebuild(qcb_server_s* s) {
         d.links_out = (char*)r->buf + r->off_out;
         d.z = (char*)r->buf + r->off_z;
         d.meas = (double*)((char*)r->buf + r->off_meas);
+        d.halves = r->off_halves ? (char*)r->buf + r->off_halves : nullptr;
         d.eps = r->eps;
         d.nb_begin = nb;
         d.nb = (int)((r->g.Vh + TILE - 1) / TILE);
@@ -328,21 +331,33 @@ bool flow_big(qcb_server_s* s, Request* r, int stage, int flip_xor, int rep) {
                    "flow launch");
 }
 
-// The small requests' measurement of one tick: batched clover pass, per-request finalize into each
-// request's slot of the device tick, tick counter advanced.  Returns the kernels launched (or -1).
-int small_measure(qcb_server_s* s, const WorkList& w, int fx) {
-    if (!cuda_ok(s, fmt_ops(s->fmt).clover_tiles(w, fx, s->partials, s->stream_small), "clover launch")) return -1;
-    k_meas_finalize<<<(unsigned)s->small.size(), 256, 0, s->stream_small>>>(s->d_desc, s->partials, s->d_tick);
+// The small requests' measurement of one tick, into each request's slot of the device tick, and the
+// tick counter advanced.  It is the measuring stage 1 of the tick's first RK3 step (clover halves;
+// a request taking its last measurement runs it too, and its flow output is left unused) and the
+// halves' per-tile sums, as qcb_flow_measure measures; without QCB_SERVE_FUSED_MEAS, a batched
+// clover pass.  Returns the kernels launched (or -1).
+int small_measure(qcb_server_s* s, const WorkList& w, int fx, int rep) {
+    const FmtOps& o = fmt_ops(s->fmt);
+    int m = 6;
+    if (QCB_SERVE_FUSED_MEAS) {
+        if (!cuda_ok(s, o.flow_tiles1_meas(w, fx, rep, s->stream_small), "flow launch")) return -1;
+        if (!cuda_ok(s, o.halves_tiles(w, s->partials, s->stream_small), "clover launch")) return -1;
+        m = 2;
+    } else if (!cuda_ok(s, o.clover_tiles(w, fx, s->partials, s->stream_small), "clover launch")) {
+        return -1;
+    }
+    k_meas_finalize<<<(unsigned)s->small.size(), 256, 0, s->stream_small>>>(s->d_desc, s->partials, s->d_tick, m);
     k_tick_bump<<<1, 1, 0, s->stream_small>>>(s->d_tick);
-    return cuda_ok(s, cudaGetLastError(), "measure finalize") ? 3 : -1;
+    return cuda_ok(s, cudaGetLastError(), "measure finalize") ? (QCB_SERVE_FUSED_MEAS ? 4 : 3) : -1;
 }
-// The small requests' n_rk RK3 steps, from buffer parity f0.
+// The small requests' n_rk RK3 steps, from buffer parity f0 (stage 1 of the first one ran in the
+// measurement).
 int small_flow(qcb_server_s* s, const WorkList& w, int f0, int rep) {
     for (int k = 0; k < s->n_rk; k++)
-        for (int stage = 1; stage <= 3; stage++)
+        for (int stage = (QCB_SERVE_FUSED_MEAS && k == 0) ? 2 : 1; stage <= 3; stage++)
             if (!cuda_ok(s, fmt_ops(s->fmt).flow(w, stage, (f0 + k) & 1, rep, s->stream_small), "flow launch"))
                 return -1;
-    return 3 * s->n_rk;
+    return 3 * s->n_rk - (QCB_SERVE_FUSED_MEAS ? 1 : 0);
 }
 
 // Runs body (small_measure or small_flow) for parity fx: plainly on the first tick of a resident
@@ -438,13 +453,15 @@ bool retire(qcb_server_s* s, const std::vector<Request*>& leaving) {
 bool big_tick(qcb_server_s* s, int rep) {
     const int fx = (int)(s->nflow_b & 1);
     bool ok = true;
-    // a big request that flows on after this measurement takes it from its next stage 1;
-    // its last measurement uses the clover pass
+    // a big request that flows on after this measurement takes it from its next stage 1; its last
+    // measurement runs a measuring stage 1 now, whose output is left unused
     for (Request* r : s->big) {
-        if (QCB_SERVE_FUSED_MEAS && s->tick_b - r->tick0 != r->n_steps - 1)
+        if (QCB_SERVE_FUSED_MEAS) {
             r->meas_slot = (double*)((char*)r->buf + r->off_meas) + (size_t)(s->tick_b - r->tick0) * 3;
-        else
+            if (s->tick_b - r->tick0 == r->n_steps - 1) ok = ok && flow_big_meas(s, r, fx, rep);
+        } else {
             ok = ok && measure_big(s, r, fx);
+        }
     }
     if (!ok) return false;
     std::vector<Request*> leaving;
@@ -474,7 +491,7 @@ bool small_tick(qcb_server_s* s, int rep) {
                                         s->stream_small), "tick counter"))
             return false;
     }
-    if (!small_run(s, s->gmeas, fx, [&] { return small_measure(s, w, fx); })) return false;
+    if (!small_run(s, s->gmeas, fx, [&] { return small_measure(s, w, fx, rep); })) return false;
     s->tick_dev = s->tick + 1;
     s->version_ticks++;
     std::vector<Request*> leaving;
@@ -641,9 +658,14 @@ int qcb_serve_submit(qcb_server s, uint64_t id, const int L[4], const double* li
     r->off_z = 2 * lb;
     r->off_meas = 2 * lb + align256(alg_bytes(s->fmt, r->g.Vh));
     r->bytes = r->off_meas + align256((size_t)n_steps * 3 * sizeof(double));
+    if (QCB_SERVE_FUSED_MEAS && !is_big(r)) {
+        r->off_halves = r->bytes;
+        r->bytes += align256(halves_bytes(s->fmt, r->g.Vh));
+    }
     if (r->bytes > s->budget) {
+        const size_t need = r->bytes;
         delete r;
-        return fail(QCB_ENOMEM, "serve submit: request needs %zu bytes, budget is %zu", r->bytes, s->budget);
+        return fail(QCB_ENOMEM, "serve submit: request needs %zu bytes, budget is %zu", need, s->budget);
     }
     {
         std::lock_guard<std::mutex> lk(s->mu);

@@ -26,6 +26,7 @@ struct LatDesc {
     int nb;           // ceil(Vh / TILE)
     int flip;         // flow: 1 if the current links sit in links_out (xor the launch's flip_xor)
     int tick0;        // serving: scheduler tick at which this lattice took its first measurement
+    void* halves;     // serving: clover halves of the measuring stage 1 (halves_bytes)
 };
 
 template <typename R, int NE>
@@ -92,7 +93,49 @@ __global__ void __launch_bounds__(QCB_FLOW_THREADS, QCB_FLOW_MINB(R))
     }
 }
 
+// Stage 1 that also writes each lattice's clover halves (the serving tick's measurement; see
+// k_flow_stage1_meas).  The links it writes are those of k_flow_tiles<R, NE, 1>.
+template <typename R, int NE>
+__global__ void __launch_bounds__(QCB_FLOW_THREADS, QCB_FLOW_MEAS_MINB(R))
+    k_flow_tiles1_meas(const LatDesc* __restrict__ lats, const int* __restrict__ tile_lat, const LatDesc one,
+                       int ntiles, int flip_xor, int reproject) {
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const LatDesc* d = lattice_of(lats, tile_lat, one, t >> 3);
+        const Geom g = d->g;
+        const int lt = t - 8 * d->nb_begin;
+        const int cls = lt & 7;
+        const int h = (lt >> 3) * TILE + threadIdx.x;
+        if (h >= g.Vh) continue;
+        const bool in_b = ((d->flip ^ flip_xor) & 1) != 0;
+        const LinkField<R, NE> win = lview<R, NE>(in_b ? d->links_out : d->links, g.Vh);
+        const LinkField<R, NE> wout = lview<R, NE>(in_b ? d->links : d->links_out, g.Vh);
+        AlgField<R> z;
+        z.p = (typename AlgField<R>::C2*)d->z;
+        z.Vh = g.Vh;
+        const HalfClovers<R> H{(R*)d->halves, 2 * g.Vh};
+        flow_link<R, NE, 1, true>(g, win, wout, z, d->eps, cls >> 1, cls & 1, h, reproject, H);
+    }
+}
+
 // ---------------------------------------------------------------- per-tile reductions
+// Clover halves -> (q, e) per tile: 2 tiles per lattice block of sites (one per parity), so the
+// per-lattice finalize sums 2 * nb partials; the per-site values are those of k_clover_halves.
+template <typename R>
+__global__ void __launch_bounds__(TILE)
+    k_halves_tiles(const LatDesc* __restrict__ lats, const int* __restrict__ tile_lat, const LatDesc one, int ntiles,
+                   double* partials) {
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const LatDesc* d = lattice_of(lats, tile_lat, one, t >> 1);
+        const int64_t Vh = d->g.Vh;
+        const int lt = t - 2 * d->nb_begin;
+        const int h = (lt >> 1) * TILE + threadIdx.x;
+        const HalfClovers<R> H{(R*)d->halves, 2 * Vh};
+        double v[3] = {0.0, 0.0, 0.0};
+        if (h < Vh) site_halves_qe(H, (int64_t)(lt & 1) * Vh + h, v);
+        block_sum_store<2>(v, partials, t);
+        __syncthreads();
+    }
+}
 // flip_xor < 0: measure `links`; otherwise measure the flow's current buffer (as above).
 // Plaquette: 2 tiles per block (one per parity); one partial per tile.
 template <typename R, int NE>

@@ -149,10 +149,11 @@ int qcb_flow_copy(qcb_flow fl, qcb_field src);
 int qcb_flow_rk3(qcb_flow fl, int n);
 /* topo_charge_flowed (src/observables/observables_mpi.cpp:159-186): copy src, then n_steps
  * times { measure (Q, E) ; if not last: n_rk RK3 steps }; tQE receives 3*n_steps doubles
- * (t, Q, E).  If plaq is non-NULL it receives n_steps plaquettes measured beside Q, E.  A
- * measurement that an RK3 step follows is taken from that step's stage 1 (the clover from the
- * force's staple differences), the last one from a clover pass; the first call with n_steps > 1 and
- * n_rk > 0 allocates the flow state's buffer for it (114 reals a site in the flow's precision). */
+ * (t, Q, E).  If plaq is non-NULL it receives n_steps plaquettes measured beside Q, E.  With
+ * n_rk > 0 every measurement is taken from a measuring RK3 stage 1 (the clover from the force's
+ * staple differences): that of the step that follows it, for the last one a stage 1 whose output
+ * is left unused; with n_rk = 0, from a clover pass.  The first call with n_rk > 0 allocates the
+ * flow state's buffer for it (114 reals a site in the flow's precision). */
 int qcb_flow_measure(qcb_flow fl, qcb_field src, int n_steps, int n_rk, double* tQE, double* plaq);
 /* The flowed field (GradientFlow::field_c); owned by the flow state. */
 qcb_field qcb_flow_field(qcb_flow fl);
@@ -271,10 +272,10 @@ int qcb_batch_tune(qcb_batch b, int n_hits, int n_trial, int allow_store_change,
  * requests of any lattice size are queued, admitted in order as the HBM budget allows, and every
  * scheduler tick measures (Q, E) of all resident requests and advances them by n_rk RK3 steps in
  * shared persistent launches.  Runs its own scheduler thread on the current device.
- * max_active <= 0: no limit besides the budget.  Besides the requests' memory (within the budget)
- * the server keeps scratch for requests of 2^17 half-sites or more, which run alone and take their
- * measurements from stage 1 as qcb_flow_measure does: 114 reals a site of the largest such
- * request, in the server's precision. */
+ * max_active <= 0: no limit besides the budget.  Every request takes its measurements from
+ * measuring RK3 stage 1 launches, as qcb_flow_measure does; a request below 2^17 half-sites holds
+ * 114 reals a site for them within its memory, and for the larger ones, which run alone, the server
+ * keeps scratch outside the budget: 114 reals a site of the largest, in the server's precision. */
 int qcb_serve_create(size_t hbm_budget_bytes, int prec, int store, int n_rk, int max_active, qcb_server* out);
 int qcb_serve_destroy(qcb_server s);
 /* Server options.  QCB_SERVE_GRAPHS (default 1): while the resident set of small requests is
