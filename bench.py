@@ -308,6 +308,9 @@ def run_reference(args, rank: int, world: int):
 
 FLOW_STEPS = 250  # t = 5.0 at eps = 0.02: the flow of the 32^4 FP64 configuration
 FLOW_COOL_S = 2.0  # idle pause before each timed flow form
+# idle pause before each serving arm: the arms are seconds of full load each, and one started right
+# after another ran 10-25% slower on some boxes (the power cap); 10 s removed that in A/B runs
+SERVE_COOL_S = 10.0
 
 
 def flow_flops_per_link_stage(prec: int) -> float:
@@ -561,7 +564,7 @@ def run_serve(qcb, n_req: int, stores=(0, 1), low_rates=(4.0, 2.0), n_low: int =
     arms = {}
     for store in stores:
         srv = qcb.Server(150 << 30, prec=qcb.PREC_F32, store=store)
-        time.sleep(FLOW_COOL_S)  # every arm starts from an idle GPU
+        time.sleep(SERVE_COOL_S)  # every arm starts from an idle GPU
         start = srv.now()
         k, done = 0, {}
         while len(done) < n_req:
@@ -594,7 +597,7 @@ def run_serve(qcb, n_req: int, stores=(0, 1), low_rates=(4.0, 2.0), n_low: int =
         fx = qcb.GaugeField((x,) * 4, 64, 0)
         serial[x] = (fx, qcb.GradientFlow(fx, 0.02, prec=64, store=0))
     tq, lat2, busy = 0.0, [], 0.0
-    time.sleep(FLOW_COOL_S)
+    time.sleep(SERVE_COOL_S)
     for i in range(n_req):
         t0 = time.perf_counter()
         f, fl = serial[int(sizes[i])]
