@@ -279,9 +279,10 @@ int qcb_batch_tune(qcb_batch b, int n_hits, int n_trial, int allow_store_change,
 int qcb_serve_create(size_t hbm_budget_bytes, int prec, int store, int n_rk, int max_active, qcb_server* out);
 int qcb_serve_destroy(qcb_server s);
 /* Server options.  QCB_SERVE_GRAPHS (default 1): while the resident set of small requests is
- * unchanged from one tick to the next, their shared launches of a tick (the batched clover pass with
- * its per-request finalize, and the n_rk RK3 steps) are replayed from CUDA graphs captured for that
- * set; 0 launches them one by one.  Results are the same either way. */
+ * unchanged from one tick to the next, their shared launches of a tick (the measuring stage 1 with
+ * the halves' sums and the per-request finalize, then the rest of the n_rk RK3 steps) are replayed
+ * from CUDA graphs captured for that set; 0 launches them one by one.  Results are the same either
+ * way. */
 #define QCB_SERVE_GRAPHS 1
 int qcb_serve_set_option(qcb_server s, int option, int value);
 /* Seconds on the server's clock (the clock of the times returned by qcb_serve_poll). */
