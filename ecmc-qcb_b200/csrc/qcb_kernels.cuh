@@ -292,7 +292,7 @@ __device__ __forceinline__ void acc_product(const M3<R>& A, const M3<R>& B, R ou
 // trace of the link's site (see above).  u is the link U_mu(x) itself.
 template <typename R, int NE>
 __device__ __forceinline__ M3<R> staple_rt_rows_meas(const Geom& g, const LinkField<R, NE>& U, const int c[4],
-                                                     int lex, int par, int mu, const M3<R>& u,
+                                                     int lex, int par, int mu, const M3<R>& u_in,
                                                      const HalfClovers<R>& H) {
     M3<R> A;
     set_zero(A);
@@ -372,6 +372,10 @@ __device__ __forceinline__ M3<R> staple_rt_rows_meas(const Geom& g, const LinkFi
             }
         }
         if (owned) {
+            // FP64: the link is reloaded here (an L1 hit) instead of held across the loop, which
+            // lets the kernel run 3 blocks/SM (measured flow 2.73-2.74 against 2.79-2.80 ms a 32^4
+            // step); FP32 holds it (no gain from the reload)
+            const M3<R> u = (sizeof(R) == 8) ? U.load_ro(mu, par, lex >> 1) : u_in;
             R tr = R(0);
 #pragma unroll
             for (int i = 0; i < 3; i++)
@@ -459,8 +463,9 @@ __device__ __forceinline__ M3<R> neg_proj_lie_mul(const M3<R>& u, const M3<R>& A
 #define QCB_FLOW1_MINB(R) (sizeof(R) == 8 ? 3 : 6)
 #endif
 // stage 1 with the clover halves: the forward staple is held until the backward one is formed
+// (FP64 3 blocks/SM with the link reloaded for the halves, no spills; FP32 4)
 #ifndef QCB_FLOW_MEAS_MINB
-#define QCB_FLOW_MEAS_MINB(R) (sizeof(R) == 8 ? 2 : 4)
+#define QCB_FLOW_MEAS_MINB(R) (sizeof(R) == 8 ? 3 : 4)
 #endif
 #ifndef QCB_FLOW_RTMU
 #define QCB_FLOW_RTMU 1
@@ -877,9 +882,15 @@ __device__ __forceinline__ void flow_link(const Geom& g, const LinkField<R, NE>&
     M3<R> F, u;
     if constexpr (MEAS) {
         // the same staple and force, with the clover halves of the input configuration
-        u = Win.load_ro(mu, par, h);
-        const M3<R> A = staple_rt_rows_meas<R, NE>(g, Win, c, lex, par, mu, u, H);
-        F = neg_proj_lie_mul(u, A);
+        if constexpr (sizeof(R) == 8) {  // the link reloaded where the halves need it
+            const M3<R> A = staple_rt_rows_meas<R, NE>(g, Win, c, lex, par, mu, u, H);
+            u = Win.load_ro(mu, par, h);
+            F = neg_proj_lie_mul(u, A);
+        } else {
+            u = Win.load_ro(mu, par, h);
+            const M3<R> A = staple_rt_rows_meas<R, NE>(g, Win, c, lex, par, mu, u, H);
+            F = neg_proj_lie_mul(u, A);
+        }
     } else if constexpr (sizeof(R) == 4 || QCB_FLOW64_ROWS) {
         // two-row staple products and the projection's entries only
         const M3<R> A = staple_rt_rows<R, NE>(g, Win, c, lex, par, mu);
